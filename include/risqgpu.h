@@ -1,0 +1,183 @@
+/*
+ * risqgpu.h -- C ABI of the B200 HCI variational hot path.
+ *
+ * One handle holds, on one GPU: the integrals, the determinant set, the sparse
+ * Hamiltonian over it and the Davidson workspace.  The entry points map onto
+ * the reference crate (aaholmes/risq) as follows:
+ *
+ *   risqgpu_create        Ham + Ints after read_ints      src/ham/read_ints.rs:73-190, src/ham/mod.rs:34-40
+ *   risqgpu_set_dets      VarWf.wf.dets / n_stored_h      src/wf/mod.rs:44-80, :1635-1683
+ *   risqgpu_build_h       gen_sparse_ham_fast_lookup /    src/var/fast_ham.rs:527-575
+ *                         gen_sparse_ham_fast             src/var/ham_gen.rs:60-292
+ *                         + sort_remove_duplicates        src/var/sparse.rs:44-56
+ *   risqgpu_sigma         MatrixOperations::matrix_vector_prod / matrix_matrix_prod
+ *                                                         src/var/sparse.rs:64-88, matrix_operations.rs:14-27
+ *   risqgpu_davidson      Davidson::new (DPR, Lowest)     src/var/eigenvalues/algorithms/davidson.rs:106-277
+ *   risqgpu_sparse_optimize  sparse_optimize              src/var/davidson.rs:43-113
+ *   risqgpu_ham_diag / risqgpu_ham_off_diag
+ *                         Ham::ham_diag / ham_off_diag_no_excite   src/ham/mod.rs:92-124, :256-303
+ *
+ * Conventions
+ *  - Determinants: uint64_t[N][4] rows {up_lo, up_hi, dn_lo, dn_hi}: the
+ *    reference's Config{up: u128, dn: u128} (src/wf/det.rs:16-19) split into
+ *    little-endian halves, bit i = spatial orbital i (0-based).
+ *  - Integrals: the reference's packed 1-based layout; one_body has
+ *    combine_2(norb+1, norb+1) entries and two_body combine_4(norb+1, ...)
+ *    entries (src/utils/ints.rs:38-68, src/ham/read_ints.rs:79-80).
+ *  - Vectors: host pointers in the caller's determinant order unless a name ends
+ *    in _device.  Block vectors are column-major: nvec columns of N doubles.
+ *  - Every function returns RISQGPU_OK (0) or an error code; nothing aborts.
+ *    risqgpu_last_error() returns a message for the last failure on a handle.
+ *  - One handle = one CUDA stream; calls are synchronous at return; a handle is
+ *    not re-entrant (the reference is single-threaded).
+ */
+#ifndef RISQGPU_H
+#define RISQGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define RISQGPU_API __attribute__((visibility("default")))
+#else
+#define RISQGPU_API
+#endif
+
+typedef struct risqgpu risqgpu_t;
+
+enum risqgpu_status {
+    RISQGPU_OK = 0,
+    RISQGPU_ERR_INVALID = 1,        /* bad argument, or call order violated */
+    RISQGPU_ERR_OOM = 2,            /* device allocation failed */
+    RISQGPU_ERR_CUDA = 3,           /* CUDA runtime error */
+    RISQGPU_ERR_NOT_CONVERGED = 4,  /* Davidson hit max_iter (DavidsonError, davidson.rs:81-90) */
+    RISQGPU_ERR_NO_DEVICE = 5,
+    RISQGPU_ERR_CAPACITY = 6        /* output buffer too small */
+};
+
+/* Storage precision of the sparse Hamiltonian values. */
+enum risqgpu_precision {
+    RISQGPU_FP64 = 0,   /* FP64 values, int32 columns */
+    RISQGPU_FP32 = 1,   /* FP32 values (rounded from FP64 Slater-Condon), int32 columns */
+    RISQGPU_MIXED = 2   /* FP32 values plus an FP32 remainder, so both FP32 and ~FP64 sigma run */
+};
+
+/* Which reference builder's rule decides the stored set (src/var/davidson.rs:55-61). */
+enum risqgpu_builder {
+    RISQGPU_BUILDER_AUTO = 0,   /* the reference's switch: N > 100 -> FAST, else LEGACY */
+    RISQGPU_BUILDER_FAST = 1,   /* fast_ham.rs: singles kept iff |H| > 1e-12, doubles iff H != 0 */
+    RISQGPU_BUILDER_LEGACY = 2  /* ham_gen.rs: every element kept iff H != 0 (spin-flip-closed sets) */
+};
+
+/* Davidson arithmetic. */
+enum risqgpu_mode {
+    RISQGPU_MODE_FP64 = 0,   /* FP64 sigma, FP64 vectors */
+    RISQGPU_MODE_MIXED = 1   /* FP32 sigma and FP32 basis; FP64 dots, Gram-Schmidt and Rayleigh-Ritz;
+                                closing FP64-sigma sweeps */
+};
+
+/* Davidson preconditioner. */
+enum risqgpu_precond {
+    RISQGPU_PRECOND_DPR = 0,      /* r / (lambda - H_ii)  (davidson.rs:391-408) */
+    RISQGPU_PRECOND_LEARNED = 1   /* DPR scaled per determinant by the loaded MLP, DPR when stalled */
+};
+
+typedef struct {
+    uint64_t n_dets;
+    uint64_t nnz_upper;       /* stored upper-triangle off-diagonal elements (the reference's count) */
+    uint64_t nnz_full;        /* both triangles as held on the device */
+    uint64_t candidates;      /* structural candidate pairs visited by the fill pass (both triangles) */
+    double ms_setup;          /* sort, grouping, partner tables */
+    double ms_count;          /* candidate count pass */
+    double ms_fill;           /* Slater-Condon + CSR fill pass */
+    double ms_total;
+    uint64_t bytes_csr;       /* bytes written for columns + values */
+} risqgpu_hstats;
+
+typedef struct {
+    int iters;                /* outer Davidson iterations */
+    int n_sigma;              /* sigma products (columns) */
+    int n_sigma_fp64;         /* of which FP64 */
+    int converged;
+    int reason;               /* 0 residual+energy, 1 tiny correction, 2 redundant vector, 3 n<=2, -1 not converged */
+    int learned_fallbacks;    /* iterations where the learned preconditioner fell back to DPR */
+    double ms_total;
+    double ms_sigma;
+    double residual[8];       /* final residual norms per root */
+} risqgpu_dstats;
+
+/* Library version string. */
+RISQGPU_API const char* risqgpu_version(void);
+
+/* Number of visible CUDA devices (0 if none or the runtime is unavailable). */
+RISQGPU_API int risqgpu_device_count(void);
+
+/* Create a handle on `device`, copying the integrals (reference packed layout). */
+RISQGPU_API int risqgpu_create(int norb, const double* one_body, size_t n1, const double* two_body, size_t n2,
+                   double e_nuc, int device, risqgpu_t** out);
+
+RISQGPU_API void risqgpu_destroy(risqgpu_t* h);
+
+RISQGPU_API const char* risqgpu_last_error(const risqgpu_t* h);
+
+/* Set the determinant set.  dets: N rows of 4 u64.  diag: the stored H_ii (the
+ * reference keeps the incrementally updated value from selection,
+ * src/wf/mod.rs:1525,1569,1618); NULL computes ham_diag on the device.
+ * n_stored_h: determinants 0..n_stored_h-1 must equal the previous call's first
+ * n_stored_h determinants; their stored elements are kept and only pairs with at
+ * least one index >= n_stored_h are built next (expand_sparse_ham_rows,
+ * src/wf/mod.rs:1664-1683).  Pass 0 for a fresh build. */
+RISQGPU_API int risqgpu_set_dets(risqgpu_t* h, const uint64_t* dets, size_t n, size_t n_stored_h, const double* diag);
+
+/* Build (or extend) the sparse Hamiltonian over the current set. */
+RISQGPU_API int risqgpu_build_h(risqgpu_t* h, int precision, int builder, risqgpu_hstats* stats);
+
+/* Stored elements after the last build. */
+RISQGPU_API int risqgpu_nnz(const risqgpu_t* h, uint64_t* nnz_upper, uint64_t* nnz_full);
+
+/* Export the stored upper triangle in the caller's determinant indices, each row
+ * sorted by column: rowptr[N+1], cols[nnz_upper], vals[nnz_upper] (FP64; the
+ * FP32 modes export their stored values widened), diag[N] (nullable). */
+RISQGPU_API int risqgpu_export_upper(risqgpu_t* h, int64_t* rowptr, int64_t* cols, double* vals, size_t cap, double* diag);
+
+/* y = H x for nvec column vectors (FP64 host buffers, caller order). */
+RISQGPU_API int risqgpu_sigma(risqgpu_t* h, const double* x, double* y, int nvec);
+
+/* Same on device buffers in the library's internal (sorted) order; dtype 0 =
+ * FP64 vectors with the FP64 (or FP32+remainder) matrix, 1 = FP32 vectors with
+ * the FP32 matrix.  Used for timing without host transfers. */
+RISQGPU_API int risqgpu_sigma_device(risqgpu_t* h, const void* x_dev, void* y_dev, int dtype);
+
+/* Lowest nroots eigenpairs.  init: N x ninit column-major (caller order) or NULL
+ * (identity columns 0 and 1, davidson.rs:318-326).  evals[nroots],
+ * evecs[N x nroots] column-major (nullable).  Returns RISQGPU_ERR_NOT_CONVERGED
+ * if max_iter passes without convergence (evals/evecs then hold the last Ritz
+ * pairs). */
+RISQGPU_API int risqgpu_davidson(risqgpu_t* h, int nroots, const double* init, int ninit, double tol, double etol,
+                     int max_iter, int mode, int precond, double* evals, double* evecs, risqgpu_dstats* stats);
+
+/* sparse_optimize (src/var/davidson.rs:43-113): build/extend H for the set, run
+ * Davidson for one root with tolerances (coeff_eps, energy_eps), write energy and
+ * coefficients.  init_coeffs NULL = no initial guess. */
+RISQGPU_API int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coeff_eps, double energy_eps,
+                            int precision, int mode, int precond, double* energy, double* coeffs,
+                            risqgpu_hstats* hstats, risqgpu_dstats* dstats);
+
+/* Element-level entry points (parity tests): H_ii and H_ij of dets[k] / (d1[k], d2[k]). */
+RISQGPU_API int risqgpu_ham_diag(risqgpu_t* h, const uint64_t* dets, size_t n, double* out);
+RISQGPU_API int risqgpu_ham_off_diag(risqgpu_t* h, const uint64_t* d1, const uint64_t* d2, size_t n, double* out);
+
+/* Learned preconditioner: load MLP weights ((2n+2) -> 128 -> 128 -> 1, FP32
+ * master copy; the device runs BF16 weights with FP32 accumulation). */
+RISQGPU_API int risqgpu_set_precond_mlp(risqgpu_t* h, int n_in, int hidden, const float* w1, const float* b1,
+                            const float* w2, const float* b2, const float* w3, const float* b3);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RISQGPU_H */

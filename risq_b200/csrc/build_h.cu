@@ -1,0 +1,944 @@
+// Sparse Hamiltonian construction on the device.
+//
+// Replaces gen_sparse_ham_fast_lookup (src/var/fast_ham.rs:527-575) and
+// gen_sparse_ham_fast (src/var/ham_gen.rs:60-292) + sort_remove_duplicates
+// (src/var/sparse.rs:44-56).  Both reference builders store the same set: every
+// pair (i, j) at excitation degree 1 or 2 with at least one index >= n_stored_h
+// whose element passes the rule (doubles: H != 0; singles: |H| > 1e-12 in the
+// fast builder, H != 0 in the legacy one, off_diag.rs:33, fast_ham.rs:505).
+//
+// Layout.  Determinants are re-ordered by (up, dn) so that every alpha group is
+// a contiguous index range; a second order by (dn, up) lists each beta group.
+// Alpha strings that differ by one electron are linked through a sorted table of
+// "string minus one electron" keys (the reference's alpha_singles,
+// fast_ham.rs:105-134).  A row's neighbours are then three index ranges:
+//   (1) its alpha group            -> beta singles and beta-beta doubles
+//   (2) its beta group             -> alpha singles and alpha-alpha doubles
+//   (3) its alpha-partner groups   -> opposite-spin doubles (beta differs by one)
+// The matrix is held with both triangles (each element is computed once per
+// side; ham_sing/ham_doub are bitwise symmetric, see bits.cuh) so sigma needs no
+// scatter.  One warp builds one row: a count pass sizes the rows, a fill pass
+// evaluates FP64 Slater-Condon and compacts the non-zeros with warp ballots.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+#include "bits.cuh"
+#include "internal.cuh"
+
+namespace risq {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__global__ void k_iota(int32_t* p, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = (int32_t)i;
+}
+
+// key[i] = src[perm[i] * stride + off]
+__global__ void k_gather_key(const uint64_t* __restrict__ src, int64_t stride, int off, const int32_t* __restrict__ perm,
+                             int64_t n, uint64_t* __restrict__ key) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        key[i] = src[(int64_t)perm[i] * stride + off];
+}
+
+// AoS caller rows -> SoA strings in sorted order, plus the two index maps.
+__global__ void k_scatter_soa(const uint64_t* __restrict__ aos, const int32_t* __restrict__ perm, int64_t n, int W,
+                              uint64_t* __restrict__ up, uint64_t* __restrict__ dn, int32_t* __restrict__ orig,
+                              int32_t* __restrict__ inv) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        int64_t c = perm[p];
+        for (int k = 0; k < W; k++) {
+            up[k * n + p] = aos[c * 4 + k];
+            dn[k * n + p] = aos[c * 4 + 2 + k];
+        }
+        orig[p] = (int32_t)c;
+        inv[c] = (int32_t)p;
+    }
+}
+
+__global__ void k_gather_f64(const double* __restrict__ src, const int32_t* __restrict__ perm, int64_t n,
+                             double* __restrict__ dst) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = src[perm[i]];
+}
+
+// Electron counts and duplicate / group-boundary flags over the sorted order.
+template <int W>
+__global__ void k_flags_alpha(const uint64_t* __restrict__ up, const uint64_t* __restrict__ dn, int64_t n, int nup,
+                              int ndn, int32_t* __restrict__ head, int* __restrict__ bad) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        int cu = 0, cd = 0;
+        bool same_up = p > 0, same_dn = p > 0;
+        for (int k = 0; k < W; k++) {
+            uint64_t u = up[k * n + p], d = dn[k * n + p];
+            cu += __popcll(u);
+            cd += __popcll(d);
+            if (p > 0) {
+                same_up = same_up && (u == up[k * n + p - 1]);
+                same_dn = same_dn && (d == dn[k * n + p - 1]);
+            }
+        }
+        if (cu != nup || cd != ndn) atomicOr(bad, 1);
+        if (same_up && same_dn) atomicOr(bad, 2);
+        head[p] = (p == 0 || !same_up) ? 1 : 0;
+    }
+}
+
+// head flags for a sorted W-word key array (SoA [W][n])
+template <int W>
+__global__ void k_flags_keys(const uint64_t* __restrict__ key, int64_t n, int32_t* __restrict__ head) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        bool same = p > 0;
+        if (p > 0)
+            for (int k = 0; k < W; k++) same = same && key[k * n + p] == key[k * n + p - 1];
+        head[p] = same ? 0 : 1;
+    }
+}
+
+// ids = inclusive_sum(head) - 1 ; start[id] = p at each head ; start[G] = n
+__global__ void k_segment_starts(const int32_t* __restrict__ incl, int64_t n, int32_t* __restrict__ ids,
+                                 int32_t* __restrict__ start) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        int id = incl[p] - 1;
+        ids[p] = id;
+        if (p == 0 || incl[p - 1] != incl[p]) start[id] = (int32_t)p;
+        if (p == n - 1) start[id + 1] = (int32_t)n;
+    }
+}
+
+// beta-ordered copies: gb[order_b[t]] = group, up_b[t] = up[order_b[t]]
+template <int W>
+__global__ void k_beta_views(const int32_t* __restrict__ order_b, const int32_t* __restrict__ gid_t,
+                             const uint64_t* __restrict__ up, int64_t n, int32_t* __restrict__ gb,
+                             uint64_t* __restrict__ up_b) {
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        int64_t p = order_b[t];
+        gb[p] = gid_t[t];
+        for (int k = 0; k < W; k++) up_b[k * n + t] = up[k * n + p];
+    }
+}
+
+// "alpha minus one electron" keys: entry e = g * nup + j removes the j-th
+// occupied orbital of unique alpha string g.
+template <int W>
+__global__ void k_remove1_keys(const uint64_t* __restrict__ up, int64_t n, const int32_t* __restrict__ ga_start,
+                               int64_t G, int nup, uint64_t* __restrict__ key) {
+    int64_t E = G * nup;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < E; e += (int64_t)gridDim.x * blockDim.x) {
+        int64_t g = e / nup;
+        int j = (int)(e % nup);
+        int64_t p = ga_start[g];
+        Bits<W> s;
+        for (int k = 0; k < W; k++) s.w[k] = up[k * n + p];
+        for (int c = 0; c < j; c++) s.pop_lowest();
+        Bits<W> full;
+        for (int k = 0; k < W; k++) full.w[k] = up[k * n + p];
+        full.clear(s.ctz());
+        for (int k = 0; k < W; k++) key[k * E + e] = full.w[k];
+    }
+}
+
+// per sorted entry: partner count (run length - 1) stored at the entry's original index
+__global__ void k_run_counts(const int32_t* __restrict__ run_id, const int32_t* __restrict__ run_start,
+                             const int32_t* __restrict__ ent, int64_t E, int32_t* __restrict__ cnt_e) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < E; s += (int64_t)gridDim.x * blockDim.x) {
+        int r = run_id[s];
+        cnt_e[ent[s]] = run_start[r + 1] - run_start[r] - 1;
+    }
+}
+
+__global__ void k_run_fill(const int32_t* __restrict__ run_id, const int32_t* __restrict__ run_start,
+                           const int32_t* __restrict__ ent, int64_t E, const int64_t* __restrict__ off_e, int nup,
+                           int32_t* __restrict__ pa_list) {
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < E; s += (int64_t)gridDim.x * blockDim.x) {
+        int r = run_id[s];
+        int64_t o = off_e[ent[s]];
+        for (int64_t y = run_start[r]; y < run_start[r + 1]; y++) {
+            if (y == s) continue;
+            pa_list[o++] = ent[y] / nup;
+        }
+    }
+}
+
+__global__ void k_pa_start(const int64_t* __restrict__ off_e, int64_t G, int nup, int64_t total,
+                           int32_t* __restrict__ pa_start) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= G; g += (int64_t)gridDim.x * blockDim.x)
+        pa_start[g] = (int32_t)(g < G ? off_e[g * nup] : total);
+}
+
+template <int W>
+struct SetView {
+    const uint64_t* __restrict__ up;
+    const uint64_t* __restrict__ dn;
+    const uint64_t* __restrict__ up_b;
+    int64_t N;
+    const int32_t* __restrict__ ga;
+    const int32_t* __restrict__ ga_start;
+    const int32_t* __restrict__ gb;
+    const int32_t* __restrict__ gb_start;
+    const int32_t* __restrict__ order_b;
+    const int32_t* __restrict__ pa_start;
+    const int32_t* __restrict__ pa_list;
+    const int32_t* __restrict__ orig;
+    int64_t nsh;
+    // previous build (incremental extension)
+    const int32_t* __restrict__ prev_inv_of_caller;  // caller -> previous internal (or null)
+    const int64_t* __restrict__ prev_row_start;
+    const int32_t* __restrict__ prev_row_len;
+    const int32_t* __restrict__ prev_cols;
+    const int32_t* __restrict__ prev_orig;
+    const int32_t* __restrict__ inv;
+    const double* __restrict__ prev_v64;
+    const float* __restrict__ prev_v32;
+    const float* __restrict__ prev_vlo;
+
+    __device__ __forceinline__ Bits<W> up_at(int64_t p) const {
+        Bits<W> b;
+#pragma unroll
+        for (int k = 0; k < W; k++) b.w[k] = __ldg(up + k * N + p);
+        return b;
+    }
+    __device__ __forceinline__ Bits<W> dn_at(int64_t p) const {
+        Bits<W> b;
+#pragma unroll
+        for (int k = 0; k < W; k++) b.w[k] = __ldg(dn + k * N + p);
+        return b;
+    }
+    __device__ __forceinline__ Bits<W> upb_at(int64_t t) const {
+        Bits<W> b;
+#pragma unroll
+        for (int k = 0; k < W; k++) b.w[k] = __ldg(up_b + k * N + t);
+        return b;
+    }
+};
+
+// MODE 0: count structural candidates per row.  MODE 1/2/3: evaluate and store
+// FP64 / FP32 / FP32 + FP32 remainder.
+template <int W, int MODE>
+__global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double thr_single, int* __restrict__ row_counter,
+                                                    int64_t* __restrict__ cnt, const int64_t* __restrict__ row_start,
+                                                    int32_t* __restrict__ row_len, int32_t* __restrict__ cols,
+                                                    double* __restrict__ v64, float* __restrict__ v32,
+                                                    float* __restrict__ vlo) {
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    for (;;) {
+        int p = 0;
+        if (lane == 0) p = atomicAdd(row_counter, 1);
+        p = __shfl_sync(FULL, p, 0);
+        if (p >= v.N) break;
+        const Bits<W> a = v.up_at(p), b = v.dn_at(p);
+        const bool p_new = v.nsh == 0 || v.orig[p] >= v.nsh;
+        int64_t base = MODE ? row_start[p] : 0;
+        int count = 0;
+
+        auto store = [&](int64_t pos, int q, double val) {
+            cols[pos] = q;
+            if (MODE == 1) v64[pos] = val;
+            if (MODE == 2) v32[pos] = (float)val;
+            if (MODE == 3) {
+                float hi = (float)val;
+                v32[pos] = hi;
+                vlo[pos] = (float)(val - (double)hi);
+            }
+        };
+        auto emit = [&](bool ok, int q, double val) {
+            unsigned m = __ballot_sync(FULL, ok);
+            if (MODE && ok) store(base + count + __popc(m & lt), q, val);
+            count += __popc(m);
+        };
+
+        // (0) elements kept from the previous build (pairs of old determinants)
+        if (!p_new && v.prev_inv_of_caller) {
+            int op = v.prev_inv_of_caller[v.orig[p]];
+            int64_t ps = v.prev_row_start[op];
+            int pl = v.prev_row_len[op];
+            if (MODE) {
+                for (int t = lane; t < pl; t += 32) {
+                    int oq = v.prev_cols[ps + t];
+                    int q = v.inv[v.prev_orig[oq]];
+                    int64_t pos = base + t;
+                    cols[pos] = q;
+                    if (MODE == 1) v64[pos] = v.prev_v64[ps + t];
+                    if (MODE == 2) v32[pos] = v.prev_v32[ps + t];
+                    if (MODE == 3) { v32[pos] = v.prev_v32[ps + t]; vlo[pos] = v.prev_vlo[ps + t]; }
+                }
+            }
+            count += pl;
+        }
+
+        // (1) same alpha string: beta singles and beta-beta doubles
+        {
+            const int g = v.ga[p];
+            const int s = v.ga_start[g], e = v.ga_start[g + 1];
+            for (int t0 = s; t0 < e; t0 += 32) {
+                const int q = t0 + lane;
+                bool ok = false;
+                double val = 0.0;
+                if (q < e && q != p) {
+                    const Bits<W> bq = v.dn_at(q);
+                    const int d = (b ^ bq).popc();
+                    if (d <= 4 && (p_new || v.orig[q] >= v.nsh)) {
+                        if (MODE == 0) ok = true;
+                        else if (d == 2) { val = sc_single<W>(I, b, bq, a); ok = fabs(val) > thr_single; }
+                        else { val = sc_double_same<W>(I, b, bq); ok = val != 0.0; }
+                    }
+                }
+                emit(ok, q, val);
+            }
+        }
+        // (2) same beta string: alpha singles and alpha-alpha doubles
+        {
+            const int g = v.gb[p];
+            const int s = v.gb_start[g], e = v.gb_start[g + 1];
+            for (int t0 = s; t0 < e; t0 += 32) {
+                const int t = t0 + lane;
+                bool ok = false;
+                double val = 0.0;
+                int q = -1;
+                if (t < e) {
+                    const Bits<W> aq = v.upb_at(t);
+                    const int d = (a ^ aq).popc();
+                    if (d != 0 && d <= 4) {
+                        q = v.order_b[t];
+                        if (p_new || v.orig[q] >= v.nsh) {
+                            if (MODE == 0) ok = true;
+                            else if (d == 2) { val = sc_single<W>(I, a, aq, b); ok = fabs(val) > thr_single; }
+                            else { val = sc_double_same<W>(I, a, aq); ok = val != 0.0; }
+                        }
+                    }
+                }
+                emit(ok, q, val);
+            }
+        }
+        // (3) alpha single-partner groups: opposite-spin doubles
+        {
+            const int g = v.ga[p];
+            const int ps = v.pa_start[g], pe = v.pa_start[g + 1];
+            for (int c0 = ps; c0 < pe; c0 += 32) {
+                const int nvalid = min(32, pe - c0);
+                int gs = 0, gl = 0;
+                if (lane < nvalid) {
+                    const int g2 = v.pa_list[c0 + lane];
+                    gs = v.ga_start[g2];
+                    gl = v.ga_start[g2 + 1] - gs;
+                }
+                int incl = gl;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int total = __shfl_sync(FULL, incl, 31);
+                const int excl = incl - gl;
+                for (int t0 = 0; t0 < total; t0 += 32) {
+                    const int my = t0 + lane;
+                    // j = number of partner groups whose inclusive end is <= my
+                    int j = 0;
+#pragma unroll
+                    for (int step = 16; step >= 1; step >>= 1) {
+                        const int vv = __shfl_sync(FULL, incl, j + step - 1);
+                        if (vv <= my) j += step;
+                    }
+                    const int gsj = __shfl_sync(FULL, gs, j);
+                    const int exj = __shfl_sync(FULL, excl, j);
+                    bool ok = false;
+                    double val = 0.0;
+                    int q = -1;
+                    if (my < total) {
+                        q = gsj + (my - exj);
+                        const Bits<W> bq = v.dn_at(q);
+                        if ((b ^ bq).popc() == 2 && (p_new || v.orig[q] >= v.nsh)) {
+                            if (MODE == 0) ok = true;
+                            else {
+                                const Bits<W> aq = v.up_at(q);
+                                val = sc_double_opp<W>(I, a, b, aq, bq);
+                                ok = val != 0.0;
+                            }
+                        }
+                    }
+                    emit(ok, q, val);
+                }
+            }
+        }
+        if (lane == 0) {
+            if (MODE == 0) cnt[p] = count;
+            else row_len[p] = count;
+        }
+    }
+}
+
+template <int W>
+__global__ void k_ham_diag(const uint64_t* __restrict__ up, const uint64_t* __restrict__ dn, int64_t n, Ints I,
+                           double* __restrict__ out) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        Bits<W> a, b;
+        for (int k = 0; k < W; k++) { a.w[k] = up[k * n + p]; b.w[k] = dn[k * n + p]; }
+        out[p] = sc_diag<W>(I, a, b);
+    }
+}
+
+// ham_off_diag_no_excite (src/ham/mod.rs:256-303) on AoS pairs, or ham_diag.
+template <int W>
+__global__ void k_ham_pairs(const uint64_t* __restrict__ d1, const uint64_t* __restrict__ d2, int64_t n, Ints I,
+                            int diag_only, double* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        Bits<W> a1, b1, a2, b2;
+        for (int k = 0; k < W; k++) {
+            a1.w[k] = d1[i * 4 + k];
+            b1.w[k] = d1[i * 4 + 2 + k];
+        }
+        if (diag_only) { out[i] = sc_diag<W>(I, a1, b1); continue; }
+        for (int k = 0; k < W; k++) {
+            a2.w[k] = d2[i * 4 + k];
+            b2.w[k] = d2[i * 4 + 2 + k];
+        }
+        bool su = a1 == a2, sd = b1 == b2;
+        double r = 0.0;
+        if (su && sd) r = 0.0;
+        else if (!su && !sd) {
+            if (a1.andnot(a2).popc() > 1 || b1.andnot(b2).popc() > 1) r = 0.0;
+            else r = sc_double_opp<W>(I, a1, b1, a2, b2);
+        } else if (su) {
+            int m = b1.andnot(b2).popc();
+            r = m > 2 ? 0.0 : (m == 1 ? sc_single<W>(I, b1, b2, a1) : sc_double_same<W>(I, b1, b2));
+        } else {
+            int m = a1.andnot(a2).popc();
+            r = m > 2 ? 0.0 : (m == 1 ? sc_single<W>(I, a1, a2, b1) : sc_double_same<W>(I, a1, a2));
+        }
+        out[i] = r;
+    }
+}
+
+inline int grid_for(risqgpu* h, int64_t n, int block = 256) {
+    int64_t g = (n + block - 1) / block;
+    int64_t cap = (int64_t)num_sms(h) * 16;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+// Stable LSD radix sort of `perm` (values) by a multi-word key.  words: list of
+// (source array, stride, offset) from least to most significant; the key of
+// element i in pass k is src[perm[i]*stride + off].
+struct KeyWord {
+    const uint64_t* src;
+    int64_t stride;
+    int off;
+    int bits;
+};
+
+int lsd_sort(risqgpu* h, int32_t*& perm, int64_t n, const std::vector<KeyWord>& words) {
+    if (n <= 1) return RISQGPU_OK;
+    uint64_t *k0 = nullptr, *k1 = nullptr;
+    int32_t* v1 = nullptr;
+    RQ_TRY(dalloc(h, k0, n));
+    RQ_TRY(dalloc(h, k1, n));
+    RQ_TRY(dalloc(h, v1, n));
+    size_t tmp_bytes = 0;
+    char* tmp = nullptr;
+    {
+        cub::DoubleBuffer<uint64_t> dk(k0, k1);
+        cub::DoubleBuffer<int32_t> dv(perm, v1);
+        cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, dk, dv, (int)n, 0, 64, h->stream);
+    }
+    int rc = dalloc(h, tmp, tmp_bytes);
+    if (rc) { dfree(k0); dfree(k1); dfree(v1); return rc; }
+    int32_t* cur = perm;
+    int32_t* alt = v1;
+    for (const KeyWord& w : words) {
+        if (w.bits <= 0) continue;
+        k_gather_key<<<grid_for(h, n), 256, 0, h->stream>>>(w.src, w.stride, w.off, cur, n, k0);
+        cub::DoubleBuffer<uint64_t> dk(k0, k1);
+        cub::DoubleBuffer<int32_t> dv(cur, alt);
+        cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, dk, dv, (int)n, 0, std::min(64, w.bits), h->stream);
+        if (dv.Current() != cur) std::swap(cur, alt);
+    }
+    int lrc = check_launch(h, "lsd_sort");
+    if (cur != perm) cudaMemcpyAsync(perm, cur, sizeof(int32_t) * n, cudaMemcpyDeviceToDevice, h->stream);
+    RQ_TRY(sync(h, "lsd_sort"));
+    dfree(k0); dfree(k1); dfree(v1);
+    dfree(tmp);
+    return lrc;
+}
+
+// head flags -> segment ids and starts; returns the number of segments
+int segments(risqgpu* h, const int32_t* head, int64_t n, int32_t* ids, int32_t*& starts, int32_t& G) {
+    int32_t* incl = nullptr;
+    RQ_TRY(dalloc(h, incl, n));
+    size_t tb = 0;
+    cub::DeviceScan::InclusiveSum(nullptr, tb, head, incl, (int)n, h->stream);
+    char* tmp = nullptr;
+    RQ_TRY(dalloc(h, tmp, tb));
+    cub::DeviceScan::InclusiveSum(tmp, tb, head, incl, (int)n, h->stream);
+    int32_t last = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&last, incl + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "segments"));
+    G = last;
+    RQ_TRY(dalloc(h, starts, (size_t)G + 1));
+    k_segment_starts<<<grid_for(h, n), 256, 0, h->stream>>>(incl, n, ids, starts);
+    RQ_TRY(check_launch(h, "segments"));
+    RQ_TRY(sync(h, "segments"));
+    dfree(incl);
+    dfree(tmp);
+    return RISQGPU_OK;
+}
+
+template <int W>
+int build_groups(risqgpu* h, const uint64_t* d_aos, const double* d_diag_in) {
+    const int64_t n = (int64_t)h->N;
+    const int norb = h->norb;
+    // (up, dn) order
+    int32_t* perm = nullptr;
+    RQ_TRY(dalloc(h, perm, n));
+    k_iota<<<grid_for(h, n), 256, 0, h->stream>>>(perm, n);
+    std::vector<KeyWord> kw;
+    for (int k = 0; k < W; k++) kw.push_back({d_aos, 4, 2 + k, norb - 64 * k});
+    for (int k = 0; k < W; k++) kw.push_back({d_aos, 4, k, norb - 64 * k});
+    RQ_TRY(lsd_sort(h, perm, n, kw));
+    RQ_TRY(dalloc(h, h->d_up, (size_t)W * n));
+    RQ_TRY(dalloc(h, h->d_dn, (size_t)W * n));
+    RQ_TRY(dalloc(h, h->d_orig, n));
+    RQ_TRY(dalloc(h, h->d_inv, n));
+    RQ_TRY(dalloc(h, h->d_diag, n));
+    k_scatter_soa<<<grid_for(h, n), 256, 0, h->stream>>>(d_aos, perm, n, W, h->d_up, h->d_dn, h->d_orig, h->d_inv);
+    Ints I{h->d_h1, h->d_h2, h->nuc};
+    if (d_diag_in) k_gather_f64<<<grid_for(h, n), 256, 0, h->stream>>>(d_diag_in, perm, n, h->d_diag);
+    else k_ham_diag<W><<<grid_for(h, n), 256, 0, h->stream>>>(h->d_up, h->d_dn, n, I, h->d_diag);
+    RQ_TRY(check_launch(h, "scatter"));
+    // alpha groups, electron-count and duplicate checks
+    int32_t* head = nullptr;
+    int* bad = nullptr;
+    RQ_TRY(dalloc(h, head, n));
+    RQ_TRY(dalloc(h, bad, 1));
+    RQ_CUDA(h, cudaMemsetAsync(bad, 0, sizeof(int), h->stream));
+    k_flags_alpha<W><<<grid_for(h, n), 256, 0, h->stream>>>(h->d_up, h->d_dn, n, h->n_up, h->n_dn, head, bad);
+    int hbad = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "flags"));
+    if (hbad & 1) { h->err = "determinants must all hold the same numbers of up and down electrons"; return RISQGPU_ERR_INVALID; }
+    if (hbad & 2) { h->err = "duplicate determinant in the set"; return RISQGPU_ERR_INVALID; }
+    RQ_TRY(dalloc(h, h->d_ga, n));
+    RQ_TRY(segments(h, head, n, h->d_ga, h->d_ga_start, h->G_a));
+    // beta order over internal indices, by (dn, up)
+    RQ_TRY(dalloc(h, h->d_order_b, n));
+    k_iota<<<grid_for(h, n), 256, 0, h->stream>>>(h->d_order_b, n);
+    std::vector<KeyWord> kb;
+    for (int k = 0; k < W; k++) kb.push_back({h->d_up + k * n, 1, 0, norb - 64 * k});
+    for (int k = 0; k < W; k++) kb.push_back({h->d_dn + k * n, 1, 0, norb - 64 * k});
+    RQ_TRY(lsd_sort(h, h->d_order_b, n, kb));
+    // beta group heads over the beta order
+    uint64_t* dnb = nullptr;
+    RQ_TRY(dalloc(h, dnb, (size_t)W * n));
+    for (int k = 0; k < W; k++)
+        k_gather_key<<<grid_for(h, n), 256, 0, h->stream>>>(h->d_dn + k * n, 1, 0, h->d_order_b, n, dnb + k * n);
+    k_flags_keys<W><<<grid_for(h, n), 256, 0, h->stream>>>(dnb, n, head);
+    RQ_TRY(check_launch(h, "beta flags"));
+    int32_t* gid_t = nullptr;
+    RQ_TRY(dalloc(h, gid_t, n));
+    RQ_TRY(segments(h, head, n, gid_t, h->d_gb_start, h->G_b));
+    RQ_TRY(dalloc(h, h->d_gb, n));
+    RQ_TRY(dalloc(h, h->d_up_b, (size_t)W * n));
+    k_beta_views<W><<<grid_for(h, n), 256, 0, h->stream>>>(h->d_order_b, gid_t, h->d_up, n, h->d_gb, h->d_up_b);
+    RQ_TRY(check_launch(h, "beta views"));
+    dfree(dnb);
+    dfree(gid_t);
+    dfree(head);
+    dfree(bad);
+    dfree(perm);
+
+    // alpha single partners through "minus one electron" keys
+    const int64_t G = h->G_a;
+    const int nup = h->n_up;
+    const int64_t E = G * nup;
+    if (E == 0) {
+        RQ_TRY(dalloc(h, h->d_pa_start, G + 1));
+        RQ_CUDA(h, cudaMemsetAsync(h->d_pa_start, 0, sizeof(int32_t) * (G + 1), h->stream));
+        RQ_TRY(dalloc(h, h->d_pa_list, 1));
+        h->n_pa = 0;
+        return sync(h, "partners");
+    }
+    uint64_t* keys = nullptr;
+    RQ_TRY(dalloc(h, keys, (size_t)W * E));
+    k_remove1_keys<W><<<grid_for(h, E), 256, 0, h->stream>>>(h->d_up, n, h->d_ga_start, G, nup, keys);
+    int32_t* ent = nullptr;
+    RQ_TRY(dalloc(h, ent, E));
+    k_iota<<<grid_for(h, E), 256, 0, h->stream>>>(ent, E);
+    std::vector<KeyWord> kr;
+    for (int k = 0; k < W; k++) kr.push_back({keys + k * E, 1, 0, norb - 64 * k});
+    RQ_TRY(lsd_sort(h, ent, E, kr));
+    uint64_t* skeys = nullptr;
+    RQ_TRY(dalloc(h, skeys, (size_t)W * E));
+    for (int k = 0; k < W; k++)
+        k_gather_key<<<grid_for(h, E), 256, 0, h->stream>>>(keys + k * E, 1, 0, ent, E, skeys + k * E);
+    int32_t* ehead = nullptr;
+    RQ_TRY(dalloc(h, ehead, E));
+    k_flags_keys<W><<<grid_for(h, E), 256, 0, h->stream>>>(skeys, E, ehead);
+    int32_t *run_id = nullptr, *run_start = nullptr;
+    int32_t R = 0;
+    RQ_TRY(dalloc(h, run_id, E));
+    RQ_TRY(segments(h, ehead, E, run_id, run_start, R));
+    int32_t* cnt_e = nullptr;
+    int64_t* off_e = nullptr;
+    RQ_TRY(dalloc(h, cnt_e, E));
+    RQ_TRY(dalloc(h, off_e, E + 1));
+    k_run_counts<<<grid_for(h, E), 256, 0, h->stream>>>(run_id, run_start, ent, E, cnt_e);
+    {
+        size_t tb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt_e, off_e, (int)E, h->stream);
+        char* tmp = nullptr;
+        RQ_TRY(dalloc(h, tmp, tb));
+        cub::DeviceScan::ExclusiveSum(tmp, tb, cnt_e, off_e, (int)E, h->stream);
+        RQ_TRY(sync(h, "partner scan"));
+        dfree(tmp);
+    }
+    int64_t last_off = 0;
+    int32_t last_cnt = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&last_off, off_e + E - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_CUDA(h, cudaMemcpyAsync(&last_cnt, cnt_e + E - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "partner total"));
+    const int64_t total = last_off + last_cnt;
+    if (total >= (int64_t)INT32_MAX) { h->err = "alpha partner table exceeds int32 range"; return RISQGPU_ERR_INVALID; }
+    h->n_pa = (size_t)total;
+    RQ_TRY(dalloc(h, h->d_pa_list, total));
+    RQ_TRY(dalloc(h, h->d_pa_start, G + 1));
+    k_run_fill<<<grid_for(h, E), 256, 0, h->stream>>>(run_id, run_start, ent, E, off_e, nup, h->d_pa_list);
+    k_pa_start<<<grid_for(h, G + 1), 256, 0, h->stream>>>(off_e, G, nup, total, h->d_pa_start);
+    RQ_TRY(check_launch(h, "partners"));
+    RQ_TRY(sync(h, "partners"));
+    dfree(keys); dfree(ent); dfree(skeys); dfree(ehead); dfree(run_id); dfree(run_start); dfree(cnt_e); dfree(off_e);
+    return RISQGPU_OK;
+}
+
+template <int W>
+SetView<W> make_view(risqgpu* h, bool with_prev, const int32_t* prev_inv_caller) {
+    SetView<W> v;
+    v.up = h->d_up; v.dn = h->d_dn; v.up_b = h->d_up_b; v.N = (int64_t)h->N;
+    v.ga = h->d_ga; v.ga_start = h->d_ga_start; v.gb = h->d_gb; v.gb_start = h->d_gb_start;
+    v.order_b = h->d_order_b; v.pa_start = h->d_pa_start; v.pa_list = h->d_pa_list;
+    v.orig = h->d_orig; v.nsh = (int64_t)h->nsh; v.inv = h->d_inv;
+    v.prev_inv_of_caller = with_prev ? prev_inv_caller : nullptr;
+    v.prev_row_start = h->d_prev_row_start; v.prev_row_len = h->d_prev_row_len; v.prev_cols = h->d_prev_cols;
+    v.prev_orig = h->d_prev_orig; v.prev_v64 = h->d_prev_val64; v.prev_v32 = h->d_prev_val32;
+    v.prev_vlo = h->d_prev_val_lo;
+    return v;
+}
+
+__global__ void k_invert(const int32_t* __restrict__ orig, int64_t n, int32_t* __restrict__ inv) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+        inv[orig[p]] = (int32_t)p;
+}
+
+template <int W>
+int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
+    using clk = std::chrono::steady_clock;
+    const int64_t n = (int64_t)h->N;
+    const bool incremental = h->nsh > 0 && h->d_prev_row_start != nullptr;
+    int32_t* prev_inv = nullptr;
+    if (incremental) {
+        RQ_TRY(dalloc(h, prev_inv, h->prev_N));
+        k_invert<<<grid_for(h, h->prev_N), 256, 0, h->stream>>>(h->d_prev_orig, (int64_t)h->prev_N, prev_inv);
+    }
+    SetView<W> v = make_view<W>(h, incremental, prev_inv);
+    Ints I{h->d_h1, h->d_h2, h->nuc};
+    int* counter = nullptr;
+    int64_t* cnt = nullptr;
+    RQ_TRY(dalloc(h, counter, 1));
+    RQ_TRY(dalloc(h, cnt, n + 1));
+    RQ_TRY(dalloc(h, h->d_row_start, n + 1));
+    RQ_TRY(dalloc(h, h->d_row_len, n));
+    const int threads = 256;
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_build_rows<W, 1>, threads, 0);
+    const int blocks = num_sms(h) * std::max(occ, 1);
+
+    RQ_TRY(sync(h, "pre-count"));
+    auto t0 = clk::now();
+    RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
+    k_build_rows<W, 0><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, cnt, nullptr, nullptr, nullptr, nullptr,
+                                                          nullptr, nullptr);
+    RQ_TRY(check_launch(h, "count rows"));
+    {
+        size_t tb = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, h->d_row_start, (int)(n + 1), h->stream);
+        char* tmp = nullptr;
+        RQ_TRY(dalloc(h, tmp, tb));
+        RQ_CUDA(h, cudaMemsetAsync(cnt + n, 0, sizeof(int64_t), h->stream));
+        cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, h->d_row_start, (int)(n + 1), h->stream);
+        RQ_TRY(sync(h, "row scan"));
+        dfree(tmp);
+    }
+    int64_t cap = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&cap, h->d_row_start + n, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "count rows"));
+    auto t1 = clk::now();
+    h->cap = (size_t)cap;
+    RQ_TRY(dalloc(h, h->d_cols, cap));
+    dfree(h->d_val64);
+    dfree(h->d_val32);
+    dfree(h->d_val_lo);
+    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, cap));
+    else RQ_TRY(dalloc(h, h->d_val32, cap));
+    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, cap));
+    RQ_TRY(sync(h, "alloc"));
+    auto t2 = clk::now();
+    RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
+    if (precision == RISQGPU_FP64)
+        k_build_rows<W, 1><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
+                                                              h->d_cols, h->d_val64, nullptr, nullptr);
+    else if (precision == RISQGPU_FP32)
+        k_build_rows<W, 2><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
+                                                              h->d_cols, nullptr, h->d_val32, nullptr);
+    else
+        k_build_rows<W, 3><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
+                                                              h->d_cols, nullptr, h->d_val32, h->d_val_lo);
+    RQ_TRY(check_launch(h, "fill rows"));
+    // stored count
+    int64_t* sum = nullptr;
+    RQ_TRY(dalloc(h, sum, 1));
+    {
+        size_t tb = 0;
+        cub::DeviceReduce::Sum(nullptr, tb, h->d_row_len, sum, (int)n, h->stream);
+        char* tmp = nullptr;
+        RQ_TRY(dalloc(h, tmp, tb));
+        cub::DeviceReduce::Sum(tmp, tb, h->d_row_len, sum, (int)n, h->stream);
+        RQ_TRY(sync(h, "fill rows"));
+        dfree(tmp);
+    }
+    auto t3 = clk::now();
+    int64_t nnz = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&nnz, sum, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "nnz"));
+    dfree(sum);
+    dfree(counter);
+    dfree(cnt);
+    dfree(prev_inv);
+    h->nnz_full = (uint64_t)nnz;
+    h->nnz_upper = (uint64_t)nnz / 2;
+    h->precision = precision;
+    if (st) {
+        st->candidates = (uint64_t)cap;
+        st->ms_count = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        st->ms_fill = std::chrono::duration<double, std::milli>(t3 - t2).count();
+        size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : 8);
+        st->bytes_csr = (uint64_t)nnz * (4 + vb);
+    }
+    return RISQGPU_OK;
+}
+
+}  // namespace
+
+void free_csr(risqgpu* h) {
+    dfree(h->d_row_start); dfree(h->d_row_len); dfree(h->d_cols);
+    dfree(h->d_val64); dfree(h->d_val32); dfree(h->d_val_lo);
+    h->built = false;
+    h->cap = 0;
+    h->nnz_full = h->nnz_upper = 0;
+}
+
+static void free_prev(risqgpu* h) {
+    dfree(h->d_prev_orig); dfree(h->d_prev_row_start); dfree(h->d_prev_row_len); dfree(h->d_prev_cols);
+    dfree(h->d_prev_val64); dfree(h->d_prev_val32); dfree(h->d_prev_val_lo);
+    h->prev_N = 0;
+    h->prev_precision = -1;
+}
+
+void free_dets(risqgpu* h) {
+    dfree(h->d_up); dfree(h->d_dn); dfree(h->d_up_b); dfree(h->d_orig); dfree(h->d_inv); dfree(h->d_diag);
+    dfree(h->d_ga); dfree(h->d_ga_start); dfree(h->d_gb); dfree(h->d_gb_start); dfree(h->d_order_b);
+    dfree(h->d_pa_start); dfree(h->d_pa_list);
+    free_csr(h);
+    free_prev(h);
+    h->N = 0;
+}
+
+static bool within_norb(const risqgpu* h, const uint64_t* d) {
+    if (h->norb >= 128) return true;
+    uint64_t m0 = h->norb >= 64 ? 0ull : (~0ull << h->norb);
+    uint64_t m1 = h->norb <= 64 ? ~0ull : (~0ull << (h->norb - 64));
+    return !((d[0] & m0) || (d[1] & m1) || (d[2] & m0) || (d[3] & m1));
+}
+
+int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const double* diag) {
+    if (!dets && n) { h->err = "dets is null"; return RISQGPU_ERR_INVALID; }
+    if (n >= (size_t)INT32_MAX) { h->err = "more than 2^31-1 determinants"; return RISQGPU_ERR_INVALID; }
+    if (nsh > n) { h->err = "n_stored_h > n"; return RISQGPU_ERR_INVALID; }
+    if (nsh > 0) {
+        if (!h->built || h->N != nsh) {
+            h->err = "n_stored_h must equal the size of the previously built set";
+            return RISQGPU_ERR_INVALID;
+        }
+        if (std::memcmp(h->h_dets.data(), dets, sizeof(uint64_t) * 4 * nsh) != 0) {
+            h->err = "the first n_stored_h determinants differ from the previous set";
+            return RISQGPU_ERR_INVALID;
+        }
+    }
+    // electron counts from the first determinant; all must agree (checked on device)
+    int nu = 0, nd = 0;
+    if (n) {
+        nu = __builtin_popcountll(dets[0]) + __builtin_popcountll(dets[1]);
+        nd = __builtin_popcountll(dets[2]) + __builtin_popcountll(dets[3]);
+    }
+    for (size_t i = 0; i < n; i++) {
+        // every orbital index must address the integral tables
+        if (!within_norb(h, dets + 4 * i)) {
+            h->err = "determinant " + std::to_string(i) + " occupies an orbital >= norb";
+            return RISQGPU_ERR_INVALID;
+        }
+    }
+    // keep the previous matrix for an incremental extension
+    if (nsh > 0) {
+        free_prev(h);
+        h->prev_N = h->N;
+        h->prev_precision = h->precision;
+        h->d_prev_orig = h->d_orig; h->d_orig = nullptr;
+        h->d_prev_row_start = h->d_row_start; h->d_row_start = nullptr;
+        h->d_prev_row_len = h->d_row_len; h->d_row_len = nullptr;
+        h->d_prev_cols = h->d_cols; h->d_cols = nullptr;
+        h->d_prev_val64 = h->d_val64; h->d_val64 = nullptr;
+        h->d_prev_val32 = h->d_val32; h->d_val32 = nullptr;
+        h->d_prev_val_lo = h->d_val_lo; h->d_val_lo = nullptr;
+        free_csr(h);
+        dfree(h->d_up); dfree(h->d_dn); dfree(h->d_up_b); dfree(h->d_inv); dfree(h->d_diag);
+        dfree(h->d_ga); dfree(h->d_ga_start); dfree(h->d_gb); dfree(h->d_gb_start); dfree(h->d_order_b);
+        dfree(h->d_pa_start); dfree(h->d_pa_list);
+        h->N = 0;
+    } else {
+        free_dets(h);
+    }
+    h->N = n;
+    h->nsh = nsh;
+    h->n_up = nu;
+    h->n_dn = nd;
+    h->h_dets.assign(dets, dets + 4 * n);
+    if (n == 0) return RISQGPU_OK;
+    uint64_t* d_aos = nullptr;
+    double* d_dg = nullptr;
+    RQ_TRY(dalloc(h, d_aos, 4 * n));
+    RQ_CUDA(h, cudaMemcpyAsync(d_aos, dets, sizeof(uint64_t) * 4 * n, cudaMemcpyHostToDevice, h->stream));
+    if (diag) {
+        RQ_TRY(dalloc(h, d_dg, n));
+        RQ_CUDA(h, cudaMemcpyAsync(d_dg, diag, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+    }
+    int rc = h->W == 1 ? build_groups<1>(h, d_aos, d_dg) : build_groups<2>(h, d_aos, d_dg);
+    RQ_TRY(sync(h, "set_dets"));
+    dfree(d_aos);
+    dfree(d_dg);
+    return rc;
+}
+
+int build_h_impl(risqgpu* h, int precision, int builder, risqgpu_hstats* st) {
+    if (precision < 0 || precision > 2) { h->err = "bad precision"; return RISQGPU_ERR_INVALID; }
+    if (builder < 0 || builder > 2) { h->err = "bad builder"; return RISQGPU_ERR_INVALID; }
+    if (h->N == 0) { h->err = "no determinants set"; return RISQGPU_ERR_INVALID; }
+    if (h->nsh > 0 && h->prev_precision != precision) {
+        h->err = "an incremental build must keep the previous build's precision";
+        return RISQGPU_ERR_INVALID;
+    }
+    bool fast = builder == RISQGPU_BUILDER_FAST || (builder == RISQGPU_BUILDER_AUTO && h->N > 100);
+    double thr = fast ? 1e-12 : 0.0;
+    auto t0 = std::chrono::steady_clock::now();
+    free_csr(h);
+    int rc = h->W == 1 ? build_rows<1>(h, precision, thr, st) : build_rows<2>(h, precision, thr, st);
+    if (rc) return rc;
+    h->built = true;
+    if (h->nsh > 0) free_prev(h);
+    h->nsh = 0;
+    if (st) {
+        st->n_dets = h->N;
+        st->nnz_upper = h->nnz_upper;
+        st->nnz_full = h->nnz_full;
+        st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return RISQGPU_OK;
+}
+
+int export_upper_impl(risqgpu* h, int64_t* rowptr, int64_t* cols, double* vals, size_t cap, double* diag) {
+    if (!h->built) { h->err = "no built matrix"; return RISQGPU_ERR_INVALID; }
+    const size_t n = h->N;
+    if (cap < h->nnz_upper) { h->err = "export capacity too small"; return RISQGPU_ERR_CAPACITY; }
+    std::vector<int64_t> rs(n + 1);
+    std::vector<int32_t> rl(n), ci(h->cap), orig(n);
+    std::vector<double> v(h->cap);
+    RQ_CUDA(h, cudaMemcpy(rs.data(), h->d_row_start, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
+    RQ_CUDA(h, cudaMemcpy(rl.data(), h->d_row_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    RQ_CUDA(h, cudaMemcpy(ci.data(), h->d_cols, sizeof(int32_t) * h->cap, cudaMemcpyDeviceToHost));
+    RQ_CUDA(h, cudaMemcpy(orig.data(), h->d_orig, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    if (h->precision == RISQGPU_FP64) {
+        RQ_CUDA(h, cudaMemcpy(v.data(), h->d_val64, sizeof(double) * h->cap, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float> hi(h->cap), lo;
+        RQ_CUDA(h, cudaMemcpy(hi.data(), h->d_val32, sizeof(float) * h->cap, cudaMemcpyDeviceToHost));
+        if (h->precision == RISQGPU_MIXED) {
+            lo.resize(h->cap);
+            RQ_CUDA(h, cudaMemcpy(lo.data(), h->d_val_lo, sizeof(float) * h->cap, cudaMemcpyDeviceToHost));
+        }
+        for (size_t k = 0; k < h->cap; k++) v[k] = (double)hi[k] + (lo.empty() ? 0.0 : (double)lo[k]);
+    }
+    // count per caller row
+    std::vector<int64_t> cnt(n + 1, 0);
+    for (size_t p = 0; p < n; p++) {
+        int64_t r = orig[p];
+        for (int64_t k = rs[p]; k < rs[p] + rl[p]; k++)
+            if (orig[ci[k]] > r) cnt[r]++;
+    }
+    rowptr[0] = 0;
+    for (size_t r = 0; r < n; r++) rowptr[r + 1] = rowptr[r] + cnt[r];
+    std::vector<int64_t> fill(rowptr, rowptr + n);
+    for (size_t p = 0; p < n; p++) {
+        int64_t r = orig[p];
+        for (int64_t k = rs[p]; k < rs[p] + rl[p]; k++) {
+            int64_t c = orig[ci[k]];
+            if (c > r) { cols[fill[r]] = c; vals[fill[r]] = v[k]; fill[r]++; }
+        }
+    }
+    std::vector<std::pair<int64_t, double>> tmp;
+    for (size_t r = 0; r < n; r++) {
+        tmp.clear();
+        for (int64_t k = rowptr[r]; k < rowptr[r + 1]; k++) tmp.emplace_back(cols[k], vals[k]);
+        std::sort(tmp.begin(), tmp.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (size_t k = 0; k < tmp.size(); k++) { cols[rowptr[r] + k] = tmp[k].first; vals[rowptr[r] + k] = tmp[k].second; }
+    }
+    if (diag) {
+        std::vector<double> dg(n);
+        RQ_CUDA(h, cudaMemcpy(dg.data(), h->d_diag, sizeof(double) * n, cudaMemcpyDeviceToHost));
+        for (size_t p = 0; p < n; p++) diag[orig[p]] = dg[p];
+    }
+    return RISQGPU_OK;
+}
+
+int ham_elements_impl(risqgpu* h, const uint64_t* d1, const uint64_t* d2, size_t n, double* out, bool diag_only) {
+    if (n == 0) return RISQGPU_OK;
+    for (size_t i = 0; i < n; i++) {
+        // every orbital index must address the integral tables
+        if (!within_norb(h, d1 + 4 * i) || (!diag_only && !within_norb(h, d2 + 4 * i))) {
+            h->err = "determinant pair " + std::to_string(i) + " occupies an orbital >= norb";
+            return RISQGPU_ERR_INVALID;
+        }
+    }
+    uint64_t *a = nullptr, *b = nullptr;
+    double* o = nullptr;
+    RQ_TRY(dalloc(h, a, 4 * n));
+    RQ_TRY(dalloc(h, o, n));
+    RQ_CUDA(h, cudaMemcpyAsync(a, d1, sizeof(uint64_t) * 4 * n, cudaMemcpyHostToDevice, h->stream));
+    if (!diag_only) {
+        RQ_TRY(dalloc(h, b, 4 * n));
+        RQ_CUDA(h, cudaMemcpyAsync(b, d2, sizeof(uint64_t) * 4 * n, cudaMemcpyHostToDevice, h->stream));
+    }
+    Ints I{h->d_h1, h->d_h2, h->nuc};
+    int grid = grid_for(h, (int64_t)n);
+    if (h->W == 1) k_ham_pairs<1><<<grid, 256, 0, h->stream>>>(a, b, (int64_t)n, I, diag_only ? 1 : 0, o);
+    else k_ham_pairs<2><<<grid, 256, 0, h->stream>>>(a, b, (int64_t)n, I, diag_only ? 1 : 0, o);
+    RQ_TRY(check_launch(h, "ham pairs"));
+    RQ_CUDA(h, cudaMemcpyAsync(out, o, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "ham pairs"));
+    dfree(a); dfree(b); dfree(o);
+    return RISQGPU_OK;
+}
+
+}  // namespace risq

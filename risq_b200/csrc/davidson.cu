@@ -1,0 +1,540 @@
+// Block Davidson on the device.
+//
+// Follows Davidson::new (src/var/eigenvalues/algorithms/davidson.rs:106-277):
+// lowest `nroots` pairs, search space nroots + 10 (Config::new, :53-79), DPR
+// correction r / (lambda - H_ii) (:391-408), orthonormalisation of each new
+// vector against the basis (MGS::orthonormalize, modified_gram_schmidt.rs:22-36),
+// restart to the Ritz vectors when the space is full (:261-269), convergence when
+// every residual norm < tol and every |lambda - lambda_prev| < etol (:179-193),
+// early exits on a correction norm < 1e-9 (:210) and on a dependent new vector
+// (:222).  The projected problem (at most 18 x 18) is solved on the host with
+// the cyclic Jacobi method (Golub & Van Loan, Matrix Computations, 8.5); the
+// reference uses nalgebra's SymmetricEigen (Householder + QR), which gives the
+// same eigenpairs to rounding.
+//
+// Device work per iteration: one fused pass for Ritz vectors, residuals and the
+// preconditioned correction; classical Gram-Schmidt applied twice (numerically
+// equivalent to MGS for these sizes, two passes over the basis instead of one
+// per column); one sigma; one pass for the new projected column.  All
+// reductions are two-stage with a fixed grid, so results are reproducible.
+// The restart takes H*ritz as the combination of the stored H*V columns rather
+// than a fresh sigma (same vector, one sigma fewer).
+//
+// MIXED mode keeps V and H*V in FP32 and runs the FP32 sigma; dots, Gram-Schmidt
+// coefficients, the projected matrix and the Ritz vectors stay FP64.  After it
+// converges, FP64-sigma sweeps (FP32 value + FP32 remainder) restart from the
+// FP64 Ritz vectors until the same criteria hold in FP64.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "internal.cuh"
+
+namespace risq {
+
+int sigma_device(risqgpu* h, const void* x, void* y, int kind);
+int mlp_scale_impl(risqgpu* h, double energy, float* out);
+
+namespace {
+
+constexpr int KMAX = 24;   // basis columns (nroots <= 8 -> at most 18)
+constexpr int RMAX = 8;    // roots
+constexpr int DBLK = 256;  // threads per reduction block
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-reduce `m` per-thread values (acc[0..m)) into partial[blockIdx.x * stride + j].
+template <int MMAX>
+__device__ __forceinline__ void block_reduce_store(double (&acc)[MMAX], int m, double* __restrict__ partial, int stride) {
+    __shared__ double sh[DBLK / 32][MMAX];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < MMAX; j++) {
+        if (j < m) {
+            double v = warp_sum_d(acc[j]);
+            if (lane == 0) sh[w][j] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x < m) {
+        double s = 0.0;
+        for (int k = 0; k < DBLK / 32; k++) s += sh[k][threadIdx.x];
+        partial[blockIdx.x * stride + threadIdx.x] = s;
+    }
+}
+
+// out[j] = sum over blocks of partial[b * stride + j], fixed order.
+__global__ void k_reduce(const double* __restrict__ partial, int nblk, int m, int stride, double* __restrict__ out) {
+    int j = blockIdx.x;
+    if (j >= m) return;
+    __shared__ double sh[DBLK];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partial[b * stride + j];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[j] = sh[0];
+}
+
+// dots[j] = <A_j, b> for j < m (A column-major, leading dimension N)
+template <typename T>
+__global__ void __launch_bounds__(DBLK) k_multidot(const T* __restrict__ A, int m, const T* __restrict__ b, int64_t N,
+                                                  double* __restrict__ partial) {
+    double acc[KMAX];
+#pragma unroll
+    for (int j = 0; j < KMAX; j++) acc[j] = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        double bi = (double)b[i];
+#pragma unroll
+        for (int j = 0; j < KMAX; j++)
+            if (j < m) acc[j] += (double)A[j * N + i] * bi;
+    }
+    block_reduce_store<KMAX>(acc, m, partial, KMAX + 1);
+}
+
+// t -= sum_j coef[j] A_j ; then partial dots <A_j, t> (j < m) and <t, t> at slot m.
+template <typename T>
+__global__ void __launch_bounds__(DBLK) k_cgs(const T* __restrict__ A, int m, T* __restrict__ t, int64_t N,
+                                             const double* __restrict__ coef, double* __restrict__ partial) {
+    __shared__ double c[KMAX];
+    if (threadIdx.x < KMAX) c[threadIdx.x] = threadIdx.x < m ? coef[threadIdx.x] : 0.0;
+    __syncthreads();
+    double acc[KMAX + 1];
+#pragma unroll
+    for (int j = 0; j <= KMAX; j++) acc[j] = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        double a[KMAX];
+        double ti = (double)t[i];
+#pragma unroll
+        for (int j = 0; j < KMAX; j++)
+            if (j < m) { a[j] = (double)A[j * N + i]; ti -= c[j] * a[j]; }
+        T tt = (T)ti;
+        t[i] = tt;
+        ti = (double)tt;
+#pragma unroll
+        for (int j = 0; j < KMAX; j++)
+            if (j < m) acc[j] += a[j] * ti;
+        acc[KMAX] += ti * ti;
+    }
+    // move the norm into slot m for the reduction
+    double out[KMAX + 1];
+#pragma unroll
+    for (int j = 0; j <= KMAX; j++) out[j] = j < m ? acc[j] : (j == m ? acc[KMAX] : 0.0);
+    block_reduce_store<KMAX + 1>(out, m + 1, partial, KMAX + 1);
+}
+
+template <typename T>
+__global__ void k_scale(T* __restrict__ t, int64_t N, const double* __restrict__ nrm2) {
+    double s = 1.0 / sqrt(*nrm2);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        t[i] = (T)((double)t[i] * s);
+}
+
+// Ritz vectors, H*ritz, residuals and the preconditioned correction for each root.
+// sm: Y (dim x nr, row-major Y[j*nr + c]) followed by lambda[nr].  Writes
+// ritz/hr (FP64, N x nr), the correction into V[:, dim + c] when `room`, and
+// partial sums: |r_c|^2 (slot c), sum_c |t_c|^2 (slot nr).
+template <typename T>
+__global__ void __launch_bounds__(DBLK) k_ritz(const T* __restrict__ V, const T* __restrict__ HV, int dim, int nr,
+                                              int64_t N, const double* __restrict__ small, const double* __restrict__ diag,
+                                              const float* __restrict__ fscale, int room, double* __restrict__ ritz,
+                                              double* __restrict__ hr, T* __restrict__ Vnew, double* __restrict__ partial) {
+    __shared__ double Y[KMAX * RMAX];
+    __shared__ double lam[RMAX];
+    for (int k = threadIdx.x; k < dim * nr; k += blockDim.x) Y[k] = small[k];
+    if (threadIdx.x < nr) lam[threadIdx.x] = small[dim * nr + threadIdx.x];
+    __syncthreads();
+    double acc[RMAX + 1];
+#pragma unroll
+    for (int c = 0; c <= RMAX; c++) acc[c] = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        double rz[RMAX], hz[RMAX];
+#pragma unroll
+        for (int c = 0; c < RMAX; c++) { rz[c] = 0.0; hz[c] = 0.0; }
+        for (int j = 0; j < dim; j++) {
+            double v = (double)V[j * N + i], hv = (double)HV[j * N + i];
+#pragma unroll
+            for (int c = 0; c < RMAX; c++)
+                if (c < nr) { rz[c] += v * Y[j * nr + c]; hz[c] += hv * Y[j * nr + c]; }
+        }
+        double d = diag[i];
+        double f = fscale ? (double)fscale[i] : 1.0;
+#pragma unroll
+        for (int c = 0; c < RMAX; c++) {
+            if (c < nr) {
+                double r = hz[c] - rz[c] * lam[c];
+                ritz[c * N + i] = rz[c];
+                hr[c * N + i] = hz[c];
+                acc[c] += r * r;
+                if (room) {
+                    double tc = r / (lam[c] - d) * f;
+                    T tt = (T)tc;
+                    Vnew[c * N + i] = tt;
+                    acc[RMAX] += (double)tt * (double)tt;
+                }
+            }
+        }
+    }
+    double out[RMAX + 1];
+#pragma unroll
+    for (int c = 0; c <= RMAX; c++) out[c] = c < nr ? acc[c] : (c == nr ? acc[RMAX] : 0.0);
+    block_reduce_store<RMAX + 1>(out, nr + 1, partial, KMAX + 1);
+}
+
+template <typename T>
+__global__ void k_set_cols(T* __restrict__ V, T* __restrict__ HV, const double* __restrict__ ritz,
+                           const double* __restrict__ hr, int nr, int64_t N) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x)
+        for (int c = 0; c < nr; c++) {
+            V[c * N + i] = (T)ritz[c * N + i];
+            if (HV) HV[c * N + i] = (T)hr[c * N + i];
+        }
+}
+
+template <typename T>
+__global__ void k_fill_init(T* __restrict__ V, int ncol, int64_t N, const double* __restrict__ src /* internal order or null */,
+                            const int32_t* __restrict__ inv, int e0, int e1) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int c = 0; c < ncol; c++) {
+            double v;
+            if (src) v = src[c * N + i];
+            else v = (i == inv[c == 0 ? e0 : e1]) ? 1.0 : 0.0;
+            V[c * N + i] = (T)v;
+        }
+    }
+}
+
+__global__ void k_to_internal(const double* __restrict__ x, const int32_t* __restrict__ orig, int64_t N, int ncol,
+                              double* __restrict__ xi) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
+        for (int c = 0; c < ncol; c++) xi[c * N + p] = x[c * N + orig[p]];
+}
+__global__ void k_to_caller(const double* __restrict__ xi, const int32_t* __restrict__ orig, int64_t N, int ncol,
+                            double* __restrict__ x) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
+        for (int c = 0; c < ncol; c++) x[c * N + orig[p]] = xi[c * N + p];
+}
+
+// Cyclic Jacobi eigen-decomposition of a symmetric n x n matrix (row-major),
+// eigenvalues ascending, Y[r*n + c] = component r of eigenvector c.
+void jacobi_sorted(int n, const double* A, double* w, double* Y) {
+    std::vector<double> a(A, A + n * n), v(n * n, 0.0);
+    for (int i = 0; i < n; i++) v[i * n + i] = 1.0;
+    for (int sweep = 0; sweep < 64; sweep++) {
+        double off = 0.0, diag = 0.0;
+        for (int i = 0; i < n; i++)
+            for (int j = 0; j < n; j++) (i == j ? diag : off) += a[i * n + j] * a[i * n + j];
+        if (off == 0.0 || off < 1e-32 * diag) break;
+        for (int p = 0; p < n - 1; p++)
+            for (int q = p + 1; q < n; q++) {
+                double apq = a[p * n + q];
+                if (apq == 0.0) continue;
+                double theta = (a[q * n + q] - a[p * n + p]) / (2.0 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+                double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < n; k++) {
+                    double x = a[k * n + p], y = a[k * n + q];
+                    a[k * n + p] = c * x - s * y;
+                    a[k * n + q] = s * x + c * y;
+                }
+                for (int k = 0; k < n; k++) {
+                    double x = a[p * n + k], y = a[q * n + k];
+                    a[p * n + k] = c * x - s * y;
+                    a[q * n + k] = s * x + c * y;
+                }
+                for (int k = 0; k < n; k++) {
+                    double x = v[k * n + p], y = v[k * n + q];
+                    v[k * n + p] = c * x - s * y;
+                    v[k * n + q] = s * x + c * y;
+                }
+            }
+    }
+    std::vector<int> idx(n);
+    for (int i = 0; i < n; i++) idx[i] = i;
+    std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return a[x * n + x] < a[y * n + y]; });
+    for (int c = 0; c < n; c++) {
+        w[c] = a[idx[c] * n + idx[c]];
+        for (int r = 0; r < n; r++) Y[r * n + c] = v[r * n + idx[c]];
+    }
+}
+
+struct Work {
+    risqgpu* h;
+    int64_t N;
+    int grid;
+    double* partial = nullptr;  // grid x (KMAX+1)
+    double* red = nullptr;      // KMAX+1
+    double* small = nullptr;    // Y + lambda
+    double* coef = nullptr;     // KMAX+1
+    int reduce(int m, double* host_out) {
+        k_reduce<<<m, DBLK, 0, h->stream>>>(partial, grid, m, KMAX + 1, red);
+        RQ_TRY(check_launch(h, "reduce"));
+        if (host_out) {
+            RQ_CUDA(h, cudaMemcpyAsync(host_out, red, sizeof(double) * m, cudaMemcpyDeviceToHost, h->stream));
+            RQ_TRY(sync(h, "reduce"));
+        }
+        return RISQGPU_OK;
+    }
+};
+
+struct LoopOut {
+    int iters = 0, n_sigma = 0, reason = -1, fallbacks = 0;
+    bool converged = false;
+    double evals[RMAX] = {0};
+    double res[RMAX] = {0};
+};
+
+// One Davidson run with basis type T.  init_int: internal-order FP64 columns (ninit)
+// or null for identity columns.  On return ritz (N x nr, FP64, internal order) holds
+// the last Ritz vectors.
+template <typename T>
+int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, const double* last_init, double tol,
+                  double etol, int max_iter, int sigma_kind, float* fscale, double* ritz, double* hr,
+                  LoopOut& out) {
+    risqgpu* h = wk.h;
+    const int64_t N = wk.N;
+    const int mss = (int64_t)(nr + 10) < N ? nr + 10 : (int)N;
+    T *V = nullptr, *HV = nullptr;
+    RQ_TRY(dalloc(h, V, (size_t)(mss + nr) * N));
+    RQ_TRY(dalloc(h, HV, (size_t)(mss + nr) * N));
+    const int g = wk.grid;
+    // initial subspace (generate_subspace, davidson.rs:318-338)
+    int dim = init_int ? ninit : std::min(2, mss);
+    if (dim > mss) dim = mss;
+    {
+        int32_t e1 = N > 1 ? 1 : 0;
+        k_fill_init<T><<<g, DBLK, 0, h->stream>>>(V, dim, N, init_int, h->d_inv, 0, e1);
+        RQ_TRY(check_launch(h, "init"));
+    }
+    // orthonormalise multi-column initial guesses (the reference's single guess is used as given)
+    if (init_int && dim > 1) {
+        for (int c = 0; c < dim; c++) {
+            T* t = V + (size_t)c * N;
+            if (c > 0) {
+                k_multidot<T><<<g, DBLK, 0, h->stream>>>(V, c, t, N, wk.partial);
+                RQ_TRY(wk.reduce(c, nullptr));
+                cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * c, cudaMemcpyDeviceToDevice, h->stream);
+                k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, c, t, N, wk.coef, wk.partial);
+                RQ_TRY(wk.reduce(c + 1, nullptr));
+                cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * (c + 1), cudaMemcpyDeviceToDevice, h->stream);
+                k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, c, t, N, wk.coef, wk.partial);
+                RQ_TRY(wk.reduce(c + 1, nullptr));
+                k_scale<T><<<g, DBLK, 0, h->stream>>>(t, N, wk.red + c);
+            } else {
+                k_multidot<T><<<g, DBLK, 0, h->stream>>>(t, 1, t, N, wk.partial);
+                RQ_TRY(wk.reduce(1, nullptr));
+                k_scale<T><<<g, DBLK, 0, h->stream>>>(t, N, wk.red);
+            }
+        }
+    }
+    for (int c = 0; c < dim; c++) RQ_TRY(sigma_device(h, V + (size_t)c * N, HV + (size_t)c * N, sigma_kind));
+    out.n_sigma += dim;
+    std::vector<double> P((size_t)KMAX * KMAX, 0.0);
+    auto proj_cols = [&](int c0, int c1, int m) -> int {  // P[i][c] for i < m, c in [c0, c1)
+        std::vector<double> col(KMAX + 1);
+        for (int c = c0; c < c1; c++) {
+            k_multidot<T><<<g, DBLK, 0, h->stream>>>(V, m, HV + (size_t)c * N, N, wk.partial);
+            RQ_TRY(wk.reduce(m, col.data()));
+            for (int i = 0; i < m; i++) { P[i * KMAX + c] = col[i]; P[c * KMAX + i] = col[i]; }
+        }
+        return RISQGPU_OK;
+    };
+    RQ_TRY(proj_cols(0, dim, dim));
+    std::vector<double> last(nr, 0.0);
+    if (last_init) for (int c = 0; c < nr; c++) last[c] = last_init[c];
+    std::vector<double> w(KMAX), Y(KMAX * KMAX), Pd(KMAX * KMAX), hostsmall(KMAX * RMAX + RMAX);
+    std::vector<double> red(KMAX + 1);
+    double e_feat = NAN;
+    std::vector<double> res_hist;
+    int it;
+    out.converged = false;
+    for (it = 0; it < max_iter; it++) {
+        for (int i = 0; i < dim; i++)
+            for (int j = 0; j < dim; j++) Pd[i * dim + j] = P[i * KMAX + j];
+        jacobi_sorted(dim, Pd.data(), w.data(), Y.data());
+        const bool room = dim + nr <= mss;
+        for (int j = 0; j < dim; j++)
+            for (int c = 0; c < nr; c++) hostsmall[j * nr + c] = Y[j * dim + c];
+        for (int c = 0; c < nr; c++) hostsmall[dim * nr + c] = w[c];
+        RQ_CUDA(h, cudaMemcpyAsync(wk.small, hostsmall.data(), sizeof(double) * (dim * nr + nr), cudaMemcpyHostToDevice,
+                                   h->stream));
+        // learned scaling: refresh the per-determinant factors when the energy used in
+        // their features moved by more than 10 mHa; fall back to plain DPR for an
+        // iteration whenever the residual did not drop by 10% over the last one
+        const float* fs = nullptr;
+        if (fscale) {
+            if (std::isnan(e_feat) || std::fabs(w[0] - e_feat) > 1e-2) {
+                e_feat = w[0];
+                RQ_TRY(mlp_scale_impl(h, e_feat, fscale));
+            }
+            const size_t k = res_hist.size();
+            bool stalled = k >= 2 && !(res_hist[k - 1] < 0.9 * res_hist[k - 2]);
+            if (stalled) out.fallbacks++;
+            else fs = fscale;
+        }
+        k_ritz<T><<<g, DBLK, 0, h->stream>>>(V, HV, dim, nr, N, wk.small, h->d_diag, fs, room ? 1 : 0, ritz, hr,
+                                             V + (size_t)dim * N, wk.partial);
+        RQ_TRY(check_launch(h, "ritz"));
+        RQ_TRY(wk.reduce(nr + 1, red.data()));
+        bool all_small = true, all_e = true;
+        res_hist.push_back(std::sqrt(red[0]));
+        for (int c = 0; c < nr; c++) {
+            out.res[c] = std::sqrt(red[c]);
+            out.evals[c] = w[c];
+            if (!(out.res[c] < tol)) all_small = false;
+            if (!(std::fabs(w[c] - last[c]) < etol)) all_e = false;
+        }
+        if (N <= 2 || (all_small && all_e)) {
+            out.converged = true;
+            out.reason = N <= 2 ? 3 : 0;
+            break;
+        }
+        for (int c = 0; c < nr; c++) last[c] = w[c];
+        if (room) {
+            if (std::sqrt(red[nr]) < 1e-9) { out.converged = true; out.reason = 1; break; }
+            bool redundant = false;
+            for (int c = 0; c < nr; c++) {
+                const int col = dim + c;
+                T* t = V + (size_t)col * N;
+                k_multidot<T><<<g, DBLK, 0, h->stream>>>(V, col, t, N, wk.partial);
+                RQ_TRY(wk.reduce(col, nullptr));
+                RQ_CUDA(h, cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * col, cudaMemcpyDeviceToDevice, h->stream));
+                k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, col, t, N, wk.coef, wk.partial);
+                RQ_TRY(wk.reduce(col + 1, nullptr));
+                RQ_CUDA(h, cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * col, cudaMemcpyDeviceToDevice, h->stream));
+                k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, col, t, N, wk.coef, wk.partial);
+                double nrm2 = 0.0;
+                k_reduce<<<col + 1, DBLK, 0, h->stream>>>(wk.partial, g, col + 1, KMAX + 1, wk.red);
+                RQ_CUDA(h, cudaMemcpyAsync(&nrm2, wk.red + col, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+                RQ_TRY(sync(h, "cgs"));
+                if (c == nr - 1 && std::sqrt(nrm2) < 1e-9) { redundant = true; break; }
+                k_scale<T><<<g, DBLK, 0, h->stream>>>(t, N, wk.red + col);
+            }
+            if (redundant) { out.converged = true; out.reason = 2; break; }
+            for (int c = 0; c < nr; c++)
+                RQ_TRY(sigma_device(h, V + (size_t)(dim + c) * N, HV + (size_t)(dim + c) * N, sigma_kind));
+            out.n_sigma += nr;
+            RQ_TRY(proj_cols(dim, dim + nr, dim + nr));
+            dim += nr;
+        } else {
+            // restart to the Ritz vectors
+            k_set_cols<T><<<g, DBLK, 0, h->stream>>>(V, HV, ritz, hr, nr, N);
+            RQ_TRY(check_launch(h, "restart"));
+            dim = nr;
+            std::fill(P.begin(), P.end(), 0.0);
+            RQ_TRY(proj_cols(0, dim, dim));
+        }
+    }
+    out.iters += it + (it < max_iter ? 1 : 0);
+    RQ_TRY(sync(h, "davidson"));
+    dfree(V);
+    dfree(HV);
+    return RISQGPU_OK;
+}
+
+}  // namespace
+
+int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double tol, double etol, int max_iter,
+                  int mode, int precond, double* evals, double* evecs, risqgpu_dstats* st) {
+    auto t0 = std::chrono::steady_clock::now();
+    if (!h->built) { h->err = "davidson before build"; return RISQGPU_ERR_INVALID; }
+    if (nroots < 1 || nroots > RMAX) { h->err = "nroots must be in [1, 8]"; return RISQGPU_ERR_INVALID; }
+    if ((size_t)nroots > h->N) { h->err = "nroots > N"; return RISQGPU_ERR_INVALID; }
+    if (init && (ninit < 1 || ninit > nroots + 10)) { h->err = "bad ninit"; return RISQGPU_ERR_INVALID; }
+    if (init && nroots > 1 && ninit < nroots) { h->err = "ninit must be >= nroots for several roots"; return RISQGPU_ERR_INVALID; }
+    if (mode == RISQGPU_MODE_MIXED && h->precision != RISQGPU_MIXED) {
+        h->err = "MIXED mode needs a MIXED build (FP32 values + FP32 remainder)";
+        return RISQGPU_ERR_INVALID;
+    }
+    if (mode == RISQGPU_MODE_FP64 && h->precision == RISQGPU_FP32) {
+        h->err = "FP64 mode needs an FP64 or MIXED build";
+        return RISQGPU_ERR_INVALID;
+    }
+    if (precond == RISQGPU_PRECOND_LEARNED && !h->mlp.loaded) {
+        h->err = "learned preconditioner requested but no MLP loaded";
+        return RISQGPU_ERR_INVALID;
+    }
+    const int64_t N = (int64_t)h->N;
+    Work wk;
+    wk.h = h;
+    wk.N = N;
+    wk.grid = std::max(1, std::min<int>((int)((N + DBLK - 1) / DBLK), num_sms(h) * 4));
+    RQ_TRY(dalloc(h, wk.partial, (size_t)wk.grid * (KMAX + 1)));
+    RQ_TRY(dalloc(h, wk.red, KMAX + 1));
+    RQ_TRY(dalloc(h, wk.small, KMAX * RMAX + RMAX));
+    RQ_TRY(dalloc(h, wk.coef, KMAX + 1));
+    double *ritz = nullptr, *hr = nullptr, *init_int = nullptr, *tmp = nullptr;
+    RQ_TRY(dalloc(h, ritz, (size_t)nroots * N));
+    RQ_TRY(dalloc(h, hr, (size_t)nroots * N));
+    int use_init = init ? std::min(ninit, nroots + 10) : 0;
+    if (init) {
+        RQ_TRY(dalloc(h, tmp, (size_t)use_init * N));
+        RQ_TRY(dalloc(h, init_int, (size_t)use_init * N));
+        RQ_CUDA(h, cudaMemcpyAsync(tmp, init, sizeof(double) * use_init * N, cudaMemcpyHostToDevice, h->stream));
+        k_to_internal<<<wk.grid, DBLK, 0, h->stream>>>(tmp, h->d_orig, N, use_init, init_int);
+        RQ_TRY(check_launch(h, "init"));
+    }
+    float* fscale = nullptr;
+    LoopOut lo;
+    int n64 = 0;
+    if (mode == RISQGPU_MODE_FP64) {
+        if (precond == RISQGPU_PRECOND_LEARNED) RQ_TRY(dalloc(h, fscale, N));
+        RQ_TRY(davidson_loop<double>(wk, nroots, init_int, use_init, nullptr, tol, etol, max_iter, 0, fscale, ritz, hr,
+                                     lo));
+        n64 = lo.n_sigma;
+    } else {
+        if (precond == RISQGPU_PRECOND_LEARNED) RQ_TRY(dalloc(h, fscale, N));
+        RQ_TRY(davidson_loop<float>(wk, nroots, init_int, use_init, nullptr, tol, etol, max_iter, 1, fscale, ritz, hr,
+                                    lo));
+        const int n32 = lo.n_sigma;
+        if (lo.converged) {
+            // closing FP64-sigma sweeps from the FP64 Ritz vectors
+            LoopOut lr;
+            double *seed = nullptr;
+            RQ_TRY(dalloc(h, seed, (size_t)nroots * N));
+            RQ_CUDA(h, cudaMemcpyAsync(seed, ritz, sizeof(double) * nroots * N, cudaMemcpyDeviceToDevice, h->stream));
+            RQ_TRY(davidson_loop<double>(wk, nroots, seed, nroots, lo.evals, tol, etol, max_iter, 0, nullptr, ritz, hr,
+                                         lr));
+            dfree(seed);
+            lr.iters += lo.iters;
+            lr.fallbacks = lo.fallbacks;
+            n64 = lr.n_sigma;
+            lr.n_sigma += n32;
+            lo = lr;
+        }
+    }
+    for (int c = 0; c < nroots; c++) evals[c] = lo.evals[c];
+    if (evecs) {
+        double* outv = nullptr;
+        RQ_TRY(dalloc(h, outv, (size_t)nroots * N));
+        k_to_caller<<<wk.grid, DBLK, 0, h->stream>>>(ritz, h->d_orig, N, nroots, outv);
+        RQ_CUDA(h, cudaMemcpyAsync(evecs, outv, sizeof(double) * nroots * N, cudaMemcpyDeviceToHost, h->stream));
+        RQ_TRY(sync(h, "evecs"));
+        dfree(outv);
+    }
+    RQ_TRY(sync(h, "davidson end"));
+    dfree(wk.partial); dfree(wk.red); dfree(wk.small); dfree(wk.coef);
+    dfree(ritz); dfree(hr); dfree(init_int); dfree(tmp); dfree(fscale);
+    if (st) {
+        st->iters = lo.iters;
+        st->n_sigma = lo.n_sigma;
+        st->n_sigma_fp64 = n64;
+        st->converged = lo.converged ? 1 : 0;
+        st->reason = lo.reason;
+        st->learned_fallbacks = lo.fallbacks;
+        for (int c = 0; c < nroots && c < 8; c++) st->residual[c] = lo.res[c];
+        st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return lo.converged ? RISQGPU_OK : RISQGPU_ERR_NOT_CONVERGED;
+}
+
+}  // namespace risq

@@ -1,0 +1,147 @@
+// sigma = H x over the stored matrix (both triangles, diagonal kept apart).
+//
+// Replaces SparseMatUpperTri::matrix_vector_prod (src/var/sparse.rs:64-78),
+// whose symmetric scatter into y[j] would need atomics on a GPU; the full
+// (both-triangle) rows make every output a private warp reduction instead.
+// One warp per row; the column/value streams are read once with evict-first
+// loads so that the gathered vector x stays resident in L2.
+#include <algorithm>
+#include <type_traits>
+
+#include "internal.cuh"
+
+namespace risq {
+
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+// VK 0: FP64 values, FP64 vectors.  VK 1: FP32 values, FP32 vectors (FP32 sums).
+// VK 2: FP32 value + FP32 remainder, FP64 vectors.  VK 3: FP32 values, FP64 vectors.
+template <int VK, typename X>
+__global__ void __launch_bounds__(256) k_spmv(int64_t N, const int64_t* __restrict__ row_start,
+                                              const int32_t* __restrict__ row_len, const int32_t* __restrict__ cols,
+                                              const double* __restrict__ v64, const float* __restrict__ v32,
+                                              const float* __restrict__ vlo, const double* __restrict__ diag,
+                                              const X* __restrict__ x, X* __restrict__ y) {
+    using A = typename std::conditional<VK == 1, float, double>::type;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t p = warp; p < N; p += nwarps) {
+        const int64_t s = row_start[p];
+        const int len = row_len[p];
+        A acc = 0;
+        int k = lane;
+        // four independent loads in flight per lane
+        for (; k + 96 < len; k += 128) {
+            int c0 = __ldcs(cols + s + k), c1 = __ldcs(cols + s + k + 32);
+            int c2 = __ldcs(cols + s + k + 64), c3 = __ldcs(cols + s + k + 96);
+            A a0, a1, a2, a3;
+            if constexpr (VK == 0) {
+                a0 = __ldcs(v64 + s + k); a1 = __ldcs(v64 + s + k + 32);
+                a2 = __ldcs(v64 + s + k + 64); a3 = __ldcs(v64 + s + k + 96);
+            } else if constexpr (VK == 2) {
+                a0 = (double)__ldcs(v32 + s + k) + (double)__ldcs(vlo + s + k);
+                a1 = (double)__ldcs(v32 + s + k + 32) + (double)__ldcs(vlo + s + k + 32);
+                a2 = (double)__ldcs(v32 + s + k + 64) + (double)__ldcs(vlo + s + k + 64);
+                a3 = (double)__ldcs(v32 + s + k + 96) + (double)__ldcs(vlo + s + k + 96);
+            } else {
+                a0 = (A)__ldcs(v32 + s + k); a1 = (A)__ldcs(v32 + s + k + 32);
+                a2 = (A)__ldcs(v32 + s + k + 64); a3 = (A)__ldcs(v32 + s + k + 96);
+            }
+            acc += a0 * (A)__ldg(x + c0);
+            acc += a1 * (A)__ldg(x + c1);
+            acc += a2 * (A)__ldg(x + c2);
+            acc += a3 * (A)__ldg(x + c3);
+        }
+        for (; k < len; k += 32) {
+            int c = __ldcs(cols + s + k);
+            A a;
+            if constexpr (VK == 0) a = __ldcs(v64 + s + k);
+            else if constexpr (VK == 2) a = (double)__ldcs(v32 + s + k) + (double)__ldcs(vlo + s + k);
+            else a = (A)__ldcs(v32 + s + k);
+            acc += a * (A)__ldg(x + c);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) y[p] = (X)(diag[p] * (double)x[p] + (double)acc);
+    }
+}
+
+__global__ void k_permute_in(const double* __restrict__ x, const int32_t* __restrict__ orig, int64_t n,
+                             double* __restrict__ xi) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+        xi[p] = x[orig[p]];
+}
+__global__ void k_permute_out(const double* __restrict__ yi, const int32_t* __restrict__ orig, int64_t n,
+                              double* __restrict__ y) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+        y[orig[p]] = yi[p];
+}
+
+}  // namespace
+
+int spmv_grid(risqgpu* h) {
+    static int cached_dev = -1, cached = 0;
+    if (cached_dev != h->device) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmv<0, double>, 256, 0);
+        cached = num_sms(h) * std::max(occ, 1);
+        cached_dev = h->device;
+    }
+    return cached;
+}
+
+int sigma_device(risqgpu* h, const void* x, void* y, int kind) {
+    if (!h->built) { h->err = "sigma before build"; return RISQGPU_ERR_INVALID; }
+    const int64_t n = (int64_t)h->N;
+    const int grid = spmv_grid(h);
+    if (kind == 0) {
+        const double* xd = (const double*)x;
+        double* yd = (double*)y;
+        if (h->precision == RISQGPU_FP64)
+            k_spmv<0, double><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, h->d_val64,
+                                                           nullptr, nullptr, h->d_diag, xd, yd);
+        else if (h->precision == RISQGPU_MIXED)
+            k_spmv<2, double><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr,
+                                                           h->d_val32, h->d_val_lo, h->d_diag, xd, yd);
+        else
+            k_spmv<3, double><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr,
+                                                           h->d_val32, nullptr, h->d_diag, xd, yd);
+    } else {
+        if (h->precision == RISQGPU_FP64) { h->err = "FP32 sigma needs an FP32 or MIXED build"; return RISQGPU_ERR_INVALID; }
+        k_spmv<1, float><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr, h->d_val32,
+                                                      nullptr, h->d_diag, (const float*)x, (float*)y);
+    }
+    return check_launch(h, "sigma");
+}
+
+int sigma_host(risqgpu* h, const double* x, double* y, int nvec) {
+    if (!h->built) { h->err = "sigma before build"; return RISQGPU_ERR_INVALID; }
+    if (nvec < 1) { h->err = "nvec < 1"; return RISQGPU_ERR_INVALID; }
+    const int64_t n = (int64_t)h->N;
+    double *dx = nullptr, *dxi = nullptr, *dyi = nullptr;
+    RQ_TRY(dalloc(h, dx, n));
+    RQ_TRY(dalloc(h, dxi, n));
+    RQ_TRY(dalloc(h, dyi, n));
+    int g = std::max(1, (int)std::min<int64_t>((n + 255) / 256, 148 * 16));
+    for (int c = 0; c < nvec; c++) {
+        RQ_CUDA(h, cudaMemcpyAsync(dx, x + (size_t)c * n, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
+        k_permute_in<<<g, 256, 0, h->stream>>>(dx, h->d_orig, n, dxi);
+        RQ_TRY(sigma_device(h, dxi, dyi, 0));
+        k_permute_out<<<g, 256, 0, h->stream>>>(dyi, h->d_orig, n, dx);
+        RQ_CUDA(h, cudaMemcpyAsync(y + (size_t)c * n, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    }
+    RQ_TRY(sync(h, "sigma_host"));
+    dfree(dx); dfree(dxi); dfree(dyi);
+    return RISQGPU_OK;
+}
+
+}  // namespace risq
