@@ -110,6 +110,19 @@ typedef struct {
     double residual[8];       /* final residual norms per root */
 } risqgpu_dstats;
 
+/* One iteration of risqgpu_variational (the loop body of variational, src/var/mod.rs:70-123). */
+typedef struct {
+    double eps;               /* selection threshold used */
+    uint64_t n_dets;          /* determinants after the iteration */
+    uint64_t n_new;           /* determinants added (with spin flips) */
+    uint64_t candidates;      /* excitations above eps not yet in the space */
+    uint64_t nnz_upper;
+    double energy;
+    int dav_iters;
+    int dav_converged;
+    double ms_select, ms_build, ms_davidson;
+} risqgpu_var_iter;
+
 /* Library version string. */
 RISQGPU_API const char* risqgpu_version(void);
 
@@ -166,6 +179,29 @@ RISQGPU_API int risqgpu_davidson(risqgpu_t* h, int nroots, const double* init, i
 RISQGPU_API int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coeff_eps, double energy_eps,
                             int precision, int mode, int precond, double* energy, double* coeffs,
                             risqgpu_hstats* hstats, risqgpu_dstats* dstats);
+
+/* HCI selection step (find_new_dets / iterate_excites, src/wf/mod.rs:1418-1631) over the
+ * current determinant set (the last risqgpu_set_dets): heat-bath expansion of every
+ * determinant with threshold eps / |coeffs[i]| (coeffs in caller order), singles only
+ * when `singles` is non-zero (the reference enables them at the target eps), new
+ * determinants in the reference's push order with spin-flipped partners
+ * (push_and_spin_flipped, src/wf/mod.rs:99-116) and their diagonal updated from the
+ * parent.  ncore: orbitals frozen by lowest h_ii (src/ham/read_ints.rs:161-184).
+ * The result stays in the handle; read it with risqgpu_get_new_dets. */
+RISQGPU_API int risqgpu_find_new_dets(risqgpu_t* h, const double* coeffs, double eps, int singles, int ncore,
+                                      size_t* n_new);
+RISQGPU_API int risqgpu_get_new_dets(risqgpu_t* h, uint64_t* dets, double* diag, size_t cap);
+
+/* The whole variational stage (init_var_wf + variational, src/wf/mod.rs:1687-1740,
+ * src/var/mod.rs:59-134) on the device: HF start, eps schedule, selection,
+ * incremental H build and Davidson each iteration.  z_sym must be 1.  max_iter: HCI
+ * iterations (the reference uses 20); dav_max_iter: Davidson iterations per solve (the
+ * reference uses 50).  The final wavefunction stays in the handle (risqgpu_get_wf). */
+RISQGPU_API int risqgpu_variational(risqgpu_t* h, int nup, int ndn, int ncore, int z_sym, double eps_var,
+                                    int max_iter, int dav_max_iter, int precision, int mode, int precond,
+                                    double* energy, uint64_t* n_dets);
+RISQGPU_API int risqgpu_get_wf(risqgpu_t* h, uint64_t* dets, double* coeffs, double* diag, size_t cap);
+RISQGPU_API int risqgpu_var_log(risqgpu_t* h, risqgpu_var_iter* out, int cap, int* n);
 
 /* Element-level entry points (parity tests): H_ii and H_ij of dets[k] / (d1[k], d2[k]). */
 RISQGPU_API int risqgpu_ham_diag(risqgpu_t* h, const uint64_t* dets, size_t n, double* out);

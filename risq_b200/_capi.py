@@ -52,6 +52,16 @@ class DStats(C.Structure):
         return d
 
 
+class VarIter(C.Structure):
+    _fields_ = [("eps", C.c_double), ("n_dets", C.c_uint64), ("n_new", C.c_uint64), ("candidates", C.c_uint64),
+                ("nnz_upper", C.c_uint64), ("energy", C.c_double), ("dav_iters", C.c_int),
+                ("dav_converged", C.c_int), ("ms_select", C.c_double), ("ms_build", C.c_double),
+                ("ms_davidson", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
 _u64p = C.POINTER(C.c_uint64)
@@ -78,6 +88,12 @@ SIGNATURES = [
     ("risqgpu_ham_diag", C.c_int, [_handle, _u64p, C.c_size_t, _dp]),
     ("risqgpu_ham_off_diag", C.c_int, [_handle, _u64p, _u64p, C.c_size_t, _dp]),
     ("risqgpu_set_precond_mlp", C.c_int, [_handle, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _fp, _fp]),
+    ("risqgpu_find_new_dets", C.c_int, [_handle, _dp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
+    ("risqgpu_get_new_dets", C.c_int, [_handle, _u64p, _dp, C.c_size_t]),
+    ("risqgpu_variational", C.c_int, [_handle, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                      C.c_int, C.c_int, C.c_int, _dp, _u64p]),
+    ("risqgpu_get_wf", C.c_int, [_handle, _u64p, _dp, _dp, C.c_size_t]),
+    ("risqgpu_var_log", C.c_int, [_handle, C.POINTER(VarIter), C.c_int, C.POINTER(C.c_int)]),
 ]
 
 _lib = None

@@ -69,6 +69,10 @@ int risqgpu_create(int norb, const double* one_body, size_t n1, const double* tw
     if (!rc) rc = dalloc(h, h->d_h2, n2);
     if (!rc && cudaMemcpy(h->d_h1, one_body, n1 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) rc = RISQGPU_ERR_CUDA;
     if (!rc && cudaMemcpy(h->d_h2, two_body, n2 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) rc = RISQGPU_ERR_CUDA;
+    if (!rc) {
+        h->h_h1.assign(one_body, one_body + n1);
+        h->h_h2.assign(two_body, two_body + n2);
+    }
     if (rc) {
         risqgpu_destroy(h);
         return rc;

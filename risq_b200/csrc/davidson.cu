@@ -297,8 +297,8 @@ struct LoopOut {
 // or null for identity columns.  On return ritz (N x nr, FP64, internal order) holds
 // the last Ritz vectors.
 template <typename T>
-int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, const double* last_init, double tol,
-                  double etol, int max_iter, int sigma_kind, float* fscale, double* ritz, double* hr,
+int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool normalize_init, const double* last_init,
+                  double tol, double etol, int max_iter, int sigma_kind, float* fscale, double* ritz, double* hr,
                   LoopOut& out) {
     risqgpu* h = wk.h;
     const int64_t N = wk.N;
@@ -315,8 +315,10 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, const dou
         k_fill_init<T><<<g, DBLK, 0, h->stream>>>(V, dim, N, init_int, h->d_inv, 0, e1);
         RQ_TRY(check_launch(h, "init"));
     }
-    // orthonormalise multi-column initial guesses (the reference's single guess is used as given)
-    if (init_int && dim > 1) {
+    // orthonormalise multi-column initial guesses; a single caller guess is used as given, as
+    // in the reference, but a guess carried over from the FP32 stage is renormalised in FP64
+    // (an FP32-rounded norm error of 1e-7 would shift the Rayleigh quotient by 1e-7 |E|)
+    if (init_int && (dim > 1 || normalize_init)) {
         for (int c = 0; c < dim; c++) {
             T* t = V + (size_t)c * N;
             if (c > 0) {
@@ -488,12 +490,12 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
     int n64 = 0;
     if (mode == RISQGPU_MODE_FP64) {
         if (precond == RISQGPU_PRECOND_LEARNED) RQ_TRY(dalloc(h, fscale, N));
-        RQ_TRY(davidson_loop<double>(wk, nroots, init_int, use_init, nullptr, tol, etol, max_iter, 0, fscale, ritz, hr,
+        RQ_TRY(davidson_loop<double>(wk, nroots, init_int, use_init, false, nullptr, tol, etol, max_iter, 0, fscale, ritz, hr,
                                      lo));
         n64 = lo.n_sigma;
     } else {
         if (precond == RISQGPU_PRECOND_LEARNED) RQ_TRY(dalloc(h, fscale, N));
-        RQ_TRY(davidson_loop<float>(wk, nroots, init_int, use_init, nullptr, tol, etol, max_iter, 1, fscale, ritz, hr,
+        RQ_TRY(davidson_loop<float>(wk, nroots, init_int, use_init, false, nullptr, tol, etol, max_iter, 1, fscale, ritz, hr,
                                     lo));
         const int n32 = lo.n_sigma;
         if (lo.converged) {
@@ -502,7 +504,7 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
             double *seed = nullptr;
             RQ_TRY(dalloc(h, seed, (size_t)nroots * N));
             RQ_CUDA(h, cudaMemcpyAsync(seed, ritz, sizeof(double) * nroots * N, cudaMemcpyDeviceToDevice, h->stream));
-            RQ_TRY(davidson_loop<double>(wk, nroots, seed, nroots, lo.evals, tol, etol, max_iter, 0, nullptr, ritz, hr,
+            RQ_TRY(davidson_loop<double>(wk, nroots, seed, nroots, true, lo.evals, tol, etol, max_iter, 0, nullptr, ritz, hr,
                                          lr));
             dfree(seed);
             lr.iters += lo.iters;

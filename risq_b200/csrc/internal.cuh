@@ -48,6 +48,7 @@ struct risqgpu {
     size_t n1 = 0, n2 = 0;
     double* d_h1 = nullptr;
     double* d_h2 = nullptr;
+    std::vector<double> h_h1, h_h2;  // host copies (excitation tables, diagonal of HF)
 
     // determinant set, internal order = sorted by (up, dn)
     int W = 1;        // 64-bit words per spin string
@@ -103,6 +104,15 @@ struct risqgpu {
     std::vector<uint64_t> h_dets;
 
     risq::MlpWeights mlp;
+
+    // variational wavefunction of the last risqgpu_variational run (caller order)
+    std::vector<uint64_t> wf_dets;
+    std::vector<double> wf_coeffs, wf_diag;
+    double wf_energy = 0.0;
+    std::vector<risqgpu_var_iter> var_log;
+    // result of the last risqgpu_find_new_dets
+    std::vector<uint64_t> pend_dets;
+    std::vector<double> pend_diag;
 };
 
 namespace risq {

@@ -160,6 +160,41 @@ class GpuHam:
         hidden, n_in = arrs[0].shape
         A.check(A.lib().risqgpu_set_precond_mlp(self._h, n_in, hidden, *[A.ptr(a, A._fp) for a in arrs]), self._h)
 
+    # --- HCI selection and the variational loop --------------------------------
+    def find_new_dets(self, coeffs, eps, singles, ncore=0):
+        """One selection step over the current set (find_new_dets, src/wf/mod.rs:1418-1631):
+        returns (new dets uint64[M, 4], their diagonals) in the reference's push order."""
+        c = np.ascontiguousarray(coeffs, dtype=np.float64)
+        if c.size != self.n:
+            raise ValueError("coefficient vector length differs from the number of determinants")
+        m = C.c_size_t()
+        A.check(A.lib().risqgpu_find_new_dets(self._h, A.ptr(c, A._dp), eps, 1 if singles else 0, ncore,
+                                              C.byref(m)), self._h)
+        d = np.zeros((m.value, 4), dtype=np.uint64)
+        g = np.zeros(m.value)
+        A.check(A.lib().risqgpu_get_new_dets(self._h, A.ptr(d, A._u64p), A.ptr(g, A._dp), m.value), self._h)
+        return d, g
+
+    def variational(self, nup, ndn, eps_var, ncore=0, max_iter=20, dav_max_iter=50, precision=A.FP64,
+                    mode=A.MODE_FP64, precond=A.PRECOND_DPR):
+        """init_var_wf + variational (src/wf/mod.rs:1687-1740, src/var/mod.rs:59-134) on the device.
+        Returns (energy, dets, coeffs, diag, log)."""
+        e = C.c_double()
+        n = C.c_uint64()
+        A.check(A.lib().risqgpu_variational(self._h, nup, ndn, ncore, 1, eps_var, max_iter, dav_max_iter, precision,
+                                            mode, precond, C.byref(e), C.byref(n)), self._h)
+        N = n.value
+        d = np.zeros((N, 4), dtype=np.uint64)
+        c = np.zeros(N)
+        g = np.zeros(N)
+        A.check(A.lib().risqgpu_get_wf(self._h, A.ptr(d, A._u64p), A.ptr(c, A._dp), A.ptr(g, A._dp), N), self._h)
+        k = C.c_int()
+        A.lib().risqgpu_var_log(self._h, None, 0, C.byref(k))
+        recs = (A.VarIter * max(k.value, 1))()
+        A.lib().risqgpu_var_log(self._h, recs, k.value, C.byref(k))
+        self.n = N
+        return e.value, d, c, g, [recs[i].as_dict() for i in range(k.value)]
+
     def sparse_optimize(self, init_coeffs=None, coeff_eps=1e-4, energy_eps=1e-8, precision=A.FP64,
                         mode=A.MODE_FP64, precond=A.PRECOND_DPR):
         """Build (or extend) H for the current set and run Davidson for the ground state.
