@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Benchmark of the HCI variational hot path (sparse H build + Davidson) on B200.
+
+Workload (default --config 1): seeded synthetic integrals n = 20 orbitals,
+8 alpha + 8 beta electrons, seed 0, HCI threshold eps_var = 5e-5.  The
+determinant set is produced, outside the timed region, by this library's own
+variational stage on the device (cached under data/).  One timed step is one
+time-to-E_var solve over that set: FP64 sparse-H build followed by plain FP64
+Davidson (DPR preconditioner, the reference's algorithm) from the reference's
+default start until |r| < 1e-4 and |dE| < 1e-8.
+
+Metric: determinants solved per second = N_dets * steps / time (max over ranks),
+whole job.  With N GPUs every rank solves its own replica (the single-GPU path
+does not shard), so scaling is weak.  Extra keys report sigma GB/s against the
+measured HBM peak, H-build elements/s, the mixed-precision solve and its |dE|.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-E_var (≤1µHa vs FP64): mixed+learned vs plain GPU; σ GB/s; H elems/s"
+CONFIGS = {
+    0: dict(n=12, nel=6, eps=1e-4),
+    1: dict(n=20, nel=8, eps=5e-5),
+    2: dict(n=24, nel=10, eps=2e-5),
+    4: dict(n=32, nel=12, eps=1e-5),
+}
+DAV_MAX_ITER = 2000  # the reference's cap of 50 does not converge on these integrals
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """SM clocks and throttle reasons sampled every 200 ms through NVML in a thread
+    (started before the warm-up so that no tool start-up lands in the timed region);
+    only samples taken between mark() and stop() are reported."""
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.t_mark = None
+        self.running = False
+
+    def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.hdl = pynvml.nvmlDeviceGetHandleByIndex(self.device)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.hdl, pynvml.NVML_CLOCK_SM)
+        except Exception as e:  # no NVML: report it instead of clocks
+            self.nv = None
+            self.err = str(e)
+            return
+        self.running = True
+        self.t = threading.Thread(target=self._loop, daemon=True)
+        self.t.start()
+
+    def _loop(self):
+        nv = self.nv
+        while self.running:
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.hdl, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.hdl)
+                self.samples.append((time.time(), mhz, r))
+            except Exception:
+                pass
+            time.sleep(0.2)
+
+    def mark(self):
+        self.t_mark = time.time()
+
+    def stop(self):
+        if self.nv is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [f"nvml unavailable: {self.err}"]}
+        self.running = False
+        self.t.join(timeout=2)
+        t1 = time.time()
+        nv = self.nv
+        names = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        win = [s for s in self.samples if self.t_mark is None or self.t_mark - 0.2 <= s[0] <= t1]
+        reasons = sorted({k for _, _, r in win for k, bit in names.items() if r & bit})
+        sm = [m for _, m, _ in win]
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": float(self.max_mhz),
+                "reasons": reasons, "samples": len(sm)}
+
+
+def det_set(cfg_id, device, log=print):
+    """The HCI determinant set of a config, made by this library's device variational stage."""
+    from risq_b200 import GpuHam, _capi
+    from risq_b200.fcidump import synthetic_integrals
+    c = CONFIGS[cfg_id]
+    ints = synthetic_integrals(c["n"], 0)
+    os.makedirs(os.path.join(ROOT, "data"), exist_ok=True)
+    path = os.path.join(ROOT, "data", f"hci_n{c['n']}_{c['nel']}_{c['eps']:g}_s0.npz")
+    if os.path.exists(path):
+        z = np.load(path, allow_pickle=True)
+        return ints, z["dets"], z["diag"], float(z["energy"]), list(z["log"])
+    t0 = time.time()
+    with GpuHam(ints, device) as g:
+        # precision -1: FP64 while the matrix fits, FP32 selection solves beyond that
+        e, dets, coeffs, diag, vlog = g.variational(c["nel"], c["nel"], c["eps"], max_iter=20,
+                                                    dav_max_iter=DAV_MAX_ITER, precision=-1)
+    log(f"# det set config {cfg_id}: N={len(dets)} E={e:.10f} ({time.time() - t0:.1f} s)")
+    for r in vlog:
+        log("#   " + json.dumps({k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()}))
+    tmp = path + f".{os.getpid()}.tmp.npz"
+    np.savez(tmp, dets=dets, diag=diag, coeffs=coeffs, energy=e, log=np.array(vlog, dtype=object))
+    os.replace(tmp, path)
+    return ints, dets, diag, e, vlog
+
+
+def cpu_sample(ints, dets, diag, vlog, budget_s=20.0):
+    """Oracle (single-threaded C restatement) time-to-E_var on a prefix of the set.
+
+    The HCI list is ordered by selection, so a prefix whose length is one of the
+    earlier iterations' sizes is that iteration's variational space; the largest
+    such prefix the CPU solves within the budget is used."""
+    from oracle import oracle as O
+    oh = O.Ham.from_arrays(ints.norb, 0, ints.nuc, ints.one_body, ints.two_body)
+    sizes = sorted({int(r["n_dets"]) for r in vlog if int(r["n_dets"]) > 2})
+    best = None
+    for n in sizes:
+        t0 = time.perf_counter()
+        sp = O.Sparse().build(oh, dets[:n], diag[:n], 0)
+        rc, ev, _, st = sp.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
+        t = time.perf_counter() - t0
+        best = dict(n=n, t=t, nnz=sp.nnz, iters=st["iters"], energy=float(ev[0]))
+        if t > budget_s / 4:
+            break
+    return best
+
+
+def run_reference(args):
+    """--impl reference: the CPU path of the reference algorithm on the host cores."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg = CONFIGS[args.config]
+    ints, dets, diag, e_gpu, vlog = det_set(args.config, 0, log=lambda *a: None)
+    times = []
+    sample = None
+    for i in range(args.warmup + args.steps):
+        s = cpu_sample(ints, dets, diag, vlog)
+        if i >= args.warmup:
+            times.append(s["t"])
+            sample = s
+    t = float(np.mean(times))
+    v = sample["n"] / t
+    out = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "dets/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"hci n{cfg['n']} {cfg['nel']}a{cfg['nel']}b eps_var {cfg['eps']:g} seed 0",
+                   "sample_prefix_dets": sample["n"], "full_dets": int(len(dets))},
+        "cpu_baseline": {"value": v, "unit": "dets/s", "cores": 1, "kind": "port",
+                         "sample": f"H build + DPR Davidson on the first {sample['n']} of {len(dets)} determinants "
+                                   f"(an earlier HCI iteration's space; {sample['nnz']} upper elements, "
+                                   f"{sample['iters']} Davidson iterations)"},
+        "e2e": {"value": v, "unit": "dets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--impl", default="risq_b200")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from risq_b200 import GpuHam, _capi
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def say(*a):
+        if rank == 0:
+            print(*a, file=sys.stderr, flush=True)
+
+    cfg = CONFIGS[args.config]
+    # every rank generates / loads its replica; rank 0 first so the others load the cache
+    if rank == 0:
+        ints, dets, diag, e_sel, vlog = det_set(args.config, local, log=say)
+    barrier()
+    if rank != 0:
+        ints, dets, diag, e_sel, vlog = det_set(args.config, local, log=lambda *a: None)
+    N = len(dets)
+    stream = torch.cuda.Stream()
+    g = GpuHam(ints, local)
+    g.set_stream(stream.cuda_stream)
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    # ---- device-resident time-to-E_var (FP64 build + plain DPR Davidson) ----
+    g.set_dets(dets, 0, diag)
+    energies, builds, davs = [], [], []
+    clocks = ClockSampler(local)
+    clocks.start()
+    for i in range(args.warmup):
+        g.build(_capi.FP64)
+        g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
+    torch.cuda.synchronize()
+    barrier()
+    clocks.mark()
+    t_start, t_end = ev(), ev()
+    t_start.record(stream)
+    for i in range(args.steps):
+        hs = g.build(_capi.FP64)
+        r = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
+        energies.append(float(r.eigenvalues[0]))
+        builds.append(hs)
+        davs.append(r.stats)
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    ms = t_start.elapsed_time(t_end) / args.steps
+    clk = clocks.stop()
+    mx = torch.tensor([ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
+    ms_max = float(mx.item())
+    barrier()
+    e64 = energies[-1]
+    dstat = davs[-1]
+    hstat = builds[-1]
+
+    # ---- end to end through the public API: host dets in, energy + coefficients out ----
+    pin = torch.empty((N, 4), dtype=torch.int64, pin_memory=True)
+    pin.numpy()[:] = dets.view(np.int64)
+    pin_diag = torch.empty(N, dtype=torch.float64, pin_memory=True)
+    pin_diag.numpy()[:] = diag
+    dets_pinned = pin.numpy().view(np.uint64)
+    e2e_ms = []
+    for i in range(max(1, min(args.steps, 3))):
+        torch.cuda.synchronize()
+        a, b = ev(), ev()
+        a.record(stream)
+        g.set_dets(dets_pinned, 0, pin_diag.numpy())
+        e_api, c_api, _, _ = g.sparse_optimize(None, 1e-4, 1e-8, max_iter=DAV_MAX_ITER)
+        b.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e = float(np.mean(e2e_ms))
+    et = torch.tensor([e2e], device="cuda")
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e = float(et.item())
+
+    # ---- sigma roofline (FP64 CSR; x, y in the library's internal order) ----
+    g.build(_capi.FP64)
+    nnz_u, nnz_f = g.nnz()
+    x = torch.randn(N, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    torch.cuda.synchronize()
+    for _ in range(3):
+        g.sigma_device(x.data_ptr(), y.data_ptr(), 0)
+    R = 20
+    a, b = ev(), ev()
+    a.record(stream)
+    for _ in range(R):
+        g.sigma_device(x.data_ptr(), y.data_ptr(), 0)
+    b.record(stream)
+    torch.cuda.synchronize()
+    t_sig = a.elapsed_time(b) / R
+    # algorithmic bytes: values + int32 columns, per row int64 start + int32 length,
+    # x and diag read once, y written once
+    b_sig = nnz_f * (8 + 4) + N * (8 + 4) + 3 * N * 8
+    peak, peak_kind = peaks()
+    sig_gbs = b_sig / (t_sig * 1e-3) / 1e9
+
+    # ---- mixed precision (FP32 sigma, FP64 dots / RR, closing FP64 sweeps) ----
+    a, b = ev(), ev()
+    a.record(stream)
+    hs_m = g.build(_capi.MIXED)
+    rm = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=_capi.MODE_MIXED)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms_mixed = a.elapsed_time(b)
+    x32 = x.float()
+    y32 = torch.empty_like(x32)
+    for _ in range(3):
+        g.sigma_device(x32.data_ptr(), y32.data_ptr(), 1)
+    a, b = ev(), ev()
+    a.record(stream)
+    for _ in range(R):
+        g.sigma_device(x32.data_ptr(), y32.data_ptr(), 1)
+    b.record(stream)
+    torch.cuda.synchronize()
+    t_sig32 = a.elapsed_time(b) / R
+    b_sig32 = nnz_f * (4 + 4) + N * (8 + 4) + N * (4 + 4 + 8)
+
+    line = {
+        "metric": METRIC,
+        "value": N * world / (ms_max * 1e-3),
+        "unit": "dets/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_max,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"hci n{cfg['n']} {cfg['nel']}a{cfg['nel']}b eps_var {cfg['eps']:g} seed 0",
+                   "n_dets": int(N), "nnz_upper": int(nnz_u), "nnz_full": int(nnz_f),
+                   "step": "FP64 sparse-H build + plain DPR Davidson to E_var (tol 1e-4, etol 1e-8)",
+                   "l2": "CSR stream larger than L2 every step", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": N * world / (e2e * 1e-3), "unit": "dets/s", "ms_per_step": e2e,
+                "h2d_bytes_per_step": int(N * 40), "d2h_bytes_per_step": int(N * 8 + 8)},
+        "roofline": {"bound": "hbm", "kernel": "k_spmv<FP64>", "achieved": sig_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": sig_gbs / peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_launch": int(b_sig), "ms_per_launch": t_sig},
+        "time_to_evar_ms": {"fp64_plain": ms_max, "mixed_dpr": ms_mixed,
+                            "dE_mixed_uHa": abs(float(rm.eigenvalues[0]) - e64) * 1e6,
+                            "fp64_iters": dstat["iters"], "mixed_iters": rm.stats["iters"],
+                            "mixed_fp64_sigmas": rm.stats["n_sigma_fp64"]},
+        "sigma": {"fp64_gbs": sig_gbs, "fp64_ms": t_sig, "fp32_gbs": b_sig32 / (t_sig32 * 1e-3) / 1e9,
+                  "fp32_ms": t_sig32, "fp32_frac": b_sig32 / (t_sig32 * 1e-3) / 1e9 / peak},
+        "h_build": {"elems_per_s": (nnz_u + N) / (hstat["ms_total"] * 1e-3), "ms": hstat["ms_total"],
+                    "gpu_ms_count": hstat["gpu_ms_count"], "gpu_ms_fill": hstat["gpu_ms_fill"],
+                    "candidates": hstat["candidates"]},
+        "davidson": {"iters": dstat["iters"], "n_sigma": dstat["n_sigma"], "ms": dstat["ms_total"],
+                     "ms_sigma": dstat["ms_sigma"], "energy": e64, "e_selection": e_sel},
+        "clocks": clk,
+        "gpu_launches": None,
+    }
+    if rank == 0 and not args.no_cpu:
+        s = cpu_sample(ints, dets, diag, vlog)
+        line["cpu_baseline"] = {"value": s["n"] / s["t"], "unit": "dets/s", "cores": 1, "kind": "port",
+                                "sample": f"oracle H build + DPR Davidson on the first {s['n']} of {N} "
+                                          f"determinants ({s['nnz']} upper elements, {s['iters']} iterations, "
+                                          f"{s['t']:.1f} s)"}
+    g.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -96,6 +96,8 @@ typedef struct {
     double ms_fill;           /* Slater-Condon + CSR fill pass */
     double ms_total;
     uint64_t bytes_csr;       /* bytes written for columns + values */
+    double gpu_ms_count;      /* CUDA-event durations on the handle's stream */
+    double gpu_ms_fill;
 } risqgpu_hstats;
 
 typedef struct {
@@ -106,7 +108,7 @@ typedef struct {
     int reason;               /* 0 residual+energy, 1 tiny correction, 2 redundant vector, 3 n<=2, -1 not converged */
     int learned_fallbacks;    /* iterations where the learned preconditioner fell back to DPR */
     double ms_total;
-    double ms_sigma;
+    double ms_sigma;          /* CUDA-event time of the sigma launches */
     double residual[8];       /* final residual norms per root */
 } risqgpu_dstats;
 
@@ -175,10 +177,16 @@ RISQGPU_API int risqgpu_davidson(risqgpu_t* h, int nroots, const double* init, i
 
 /* sparse_optimize (src/var/davidson.rs:43-113): build/extend H for the set, run
  * Davidson for one root with tolerances (coeff_eps, energy_eps), write energy and
- * coefficients.  init_coeffs NULL = no initial guess. */
+ * coefficients.  init_coeffs NULL = no initial guess.  max_iter: Davidson iterations
+ * (the reference fixes 50, algorithms/davidson.rs:73). */
 RISQGPU_API int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coeff_eps, double energy_eps,
-                            int precision, int mode, int precond, double* energy, double* coeffs,
+                            int max_iter, int precision, int mode, int precond, double* energy, double* coeffs,
                             risqgpu_hstats* hstats, risqgpu_dstats* dstats);
+
+/* Run the handle's work on `stream` (a cudaStream_t on the handle's device; NULL
+ * restores the handle's own stream), so that a caller can order and time it with
+ * its own events. */
+RISQGPU_API int risqgpu_set_stream(risqgpu_t* h, void* stream);
 
 /* HCI selection step (find_new_dets / iterate_excites, src/wf/mod.rs:1418-1631) over the
  * current determinant set (the last risqgpu_set_dets): heat-bath expansion of every

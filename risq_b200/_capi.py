@@ -35,7 +35,8 @@ STATUS_NAMES = {
 class HStats(C.Structure):
     _fields_ = [("n_dets", C.c_uint64), ("nnz_upper", C.c_uint64), ("nnz_full", C.c_uint64),
                 ("candidates", C.c_uint64), ("ms_setup", C.c_double), ("ms_count", C.c_double),
-                ("ms_fill", C.c_double), ("ms_total", C.c_double), ("bytes_csr", C.c_uint64)]
+                ("ms_fill", C.c_double), ("ms_total", C.c_double), ("bytes_csr", C.c_uint64),
+                ("gpu_ms_count", C.c_double), ("gpu_ms_fill", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -83,8 +84,9 @@ SIGNATURES = [
     ("risqgpu_sigma_device", C.c_int, [_handle, C.c_void_p, C.c_void_p, C.c_int]),
     ("risqgpu_davidson", C.c_int, [_handle, C.c_int, _dp, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
                                    _dp, _dp, C.POINTER(DStats)]),
-    ("risqgpu_sparse_optimize", C.c_int, [_handle, _dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, _dp, _dp,
-                                          C.POINTER(HStats), C.POINTER(DStats)]),
+    ("risqgpu_sparse_optimize", C.c_int, [_handle, _dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                          _dp, _dp, C.POINTER(HStats), C.POINTER(DStats)]),
+    ("risqgpu_set_stream", C.c_int, [_handle, C.c_void_p]),
     ("risqgpu_ham_diag", C.c_int, [_handle, _u64p, C.c_size_t, _dp]),
     ("risqgpu_ham_off_diag", C.c_int, [_handle, _u64p, _u64p, C.c_size_t, _dp]),
     ("risqgpu_set_precond_mlp", C.c_int, [_handle, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _fp, _fp]),

@@ -658,10 +658,14 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     const int blocks = num_sms(h) * std::max(occ, 1);
 
     RQ_TRY(sync(h, "pre-count"));
+    cudaEvent_t ev[4];
+    for (auto& e : ev) RQ_CUDA(h, cudaEventCreate(&e));
     auto t0 = clk::now();
     RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
+    RQ_CUDA(h, cudaEventRecord(ev[0], h->stream));
     k_build_rows<W, 0><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, cnt, nullptr, nullptr, nullptr, nullptr,
                                                           nullptr, nullptr);
+    RQ_CUDA(h, cudaEventRecord(ev[1], h->stream));
     RQ_TRY(check_launch(h, "count rows"));
     {
         size_t tb = 0;
@@ -677,6 +681,21 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     RQ_CUDA(h, cudaMemcpyAsync(&cap, h->d_row_start + n, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
     RQ_TRY(sync(h, "count rows"));
     auto t1 = clk::now();
+    {
+        // refuse up front when the rows cannot be stored, leaving the handle unchanged
+        size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : 8);
+        size_t need = (size_t)cap * (4 + vb) + ((size_t)64 << 20);
+        size_t fr = 0, tot = 0;
+        RQ_CUDA(h, cudaMemGetInfo(&fr, &tot));
+        if (need > fr) {
+            h->err = "sparse H needs " + std::to_string(need >> 20) + " MiB, " + std::to_string(fr >> 20) +
+                     " MiB free";
+            dfree(counter);
+            dfree(cnt);
+            dfree(prev_inv);
+            return RISQGPU_ERR_OOM;
+        }
+    }
     h->cap = (size_t)cap;
     RQ_TRY(dalloc(h, h->d_cols, cap));
     dfree(h->d_val64);
@@ -688,6 +707,7 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     RQ_TRY(sync(h, "alloc"));
     auto t2 = clk::now();
     RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
+    RQ_CUDA(h, cudaEventRecord(ev[2], h->stream));
     if (precision == RISQGPU_FP64)
         k_build_rows<W, 1><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
                                                               h->d_cols, h->d_val64, nullptr, nullptr);
@@ -697,6 +717,7 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     else
         k_build_rows<W, 3><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
                                                               h->d_cols, nullptr, h->d_val32, h->d_val_lo);
+    RQ_CUDA(h, cudaEventRecord(ev[3], h->stream));
     RQ_TRY(check_launch(h, "fill rows"));
     // stored count
     int64_t* sum = nullptr;
@@ -721,7 +742,13 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     h->nnz_full = (uint64_t)nnz;
     h->nnz_upper = (uint64_t)nnz / 2;
     h->precision = precision;
+    float ms_c = 0.f, ms_f = 0.f;
+    cudaEventElapsedTime(&ms_c, ev[0], ev[1]);
+    cudaEventElapsedTime(&ms_f, ev[2], ev[3]);
+    for (auto& e : ev) cudaEventDestroy(e);
     if (st) {
+        st->gpu_ms_count = ms_c;
+        st->gpu_ms_fill = ms_f;
         st->candidates = (uint64_t)cap;
         st->ms_count = std::chrono::duration<double, std::milli>(t1 - t0).count();
         st->ms_fill = std::chrono::duration<double, std::milli>(t3 - t2).count();

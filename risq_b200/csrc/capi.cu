@@ -64,7 +64,8 @@ int risqgpu_create(int norb, const double* one_body, size_t n1, const double* tw
     h->n1 = n1;
     h->n2 = n2;
     int rc = RISQGPU_OK;
-    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) rc = RISQGPU_ERR_CUDA;
+    if (cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking) != cudaSuccess) rc = RISQGPU_ERR_CUDA;
+    h->stream = h->own_stream;
     if (!rc) rc = dalloc(h, h->d_h1, n1);
     if (!rc) rc = dalloc(h, h->d_h2, n2);
     if (!rc && cudaMemcpy(h->d_h1, one_body, n1 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) rc = RISQGPU_ERR_CUDA;
@@ -89,7 +90,7 @@ void risqgpu_destroy(risqgpu_t* h) {
     free_mlp(h);
     dfree(h->d_h1);
     dfree(h->d_h2);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
 }
 
@@ -145,10 +146,10 @@ int risqgpu_davidson(risqgpu_t* h, int nroots, const double* init, int ninit, do
     return davidson_impl(h, nroots, init, ninit, tol, etol, max_iter, mode, precond, evals, evecs, stats);
 }
 
-int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coeff_eps, double energy_eps, int precision,
-                            int mode, int precond, double* energy, double* coeffs, risqgpu_hstats* hstats,
-                            risqgpu_dstats* dstats) {
-    if (!h || !energy || !coeffs) return RISQGPU_ERR_INVALID;
+int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coeff_eps, double energy_eps,
+                            int max_iter, int precision, int mode, int precond, double* energy, double* coeffs,
+                            risqgpu_hstats* hstats, risqgpu_dstats* dstats) {
+    if (!h || !energy || !coeffs || max_iter < 1) return RISQGPU_ERR_INVALID;
     DeviceGuard g(h->device);
     if (hstats) std::memset(hstats, 0, sizeof(*hstats));
     if (dstats) std::memset(dstats, 0, sizeof(*dstats));
@@ -156,8 +157,8 @@ int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coef
     if (rc) return rc;
     double e = 0.0;
     std::vector<double> v(h->N);
-    rc = davidson_impl(h, 1, init_coeffs, init_coeffs ? 1 : 0, coeff_eps, energy_eps, 50, mode, precond, &e, v.data(),
-                       dstats);
+    rc = davidson_impl(h, 1, init_coeffs, init_coeffs ? 1 : 0, coeff_eps, energy_eps, max_iter, mode, precond, &e,
+                       v.data(), dstats);
     if (rc == RISQGPU_ERR_NOT_CONVERGED) {
         h->err = "Davidson Algorithm did not converge!";
         return rc;  // energy and coefficients are left unchanged (var/davidson.rs:109-111)
@@ -165,6 +166,14 @@ int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coef
     if (rc) return rc;
     *energy = e;
     std::memcpy(coeffs, v.data(), sizeof(double) * h->N);
+    return RISQGPU_OK;
+}
+
+int risqgpu_set_stream(risqgpu_t* h, void* stream) {
+    if (!h) return RISQGPU_ERR_INVALID;
+    DeviceGuard g(h->device);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return RISQGPU_ERR_CUDA;
+    h->stream = stream ? (cudaStream_t)stream : h->own_stream;
     return RISQGPU_OK;
 }
 

@@ -39,6 +39,23 @@ int mlp_scale_impl(risqgpu* h, double energy, float* out);
 
 namespace {
 
+// sigma with CUDA-event timing accumulated into the handle
+int timed_sigma(risqgpu* h, const void* x, void* y, int kind) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, h->stream);
+    int rc = sigma_device(h, x, y, kind);
+    cudaEventRecord(b, h->stream);
+    cudaEventSynchronize(b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    h->sigma_ms_acc += ms;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return rc;
+}
+
 constexpr int KMAX = 24;   // basis columns (nroots <= 8 -> at most 18)
 constexpr int RMAX = 8;    // roots
 constexpr int DBLK = 256;  // threads per reduction block
@@ -338,7 +355,7 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
             }
         }
     }
-    for (int c = 0; c < dim; c++) RQ_TRY(sigma_device(h, V + (size_t)c * N, HV + (size_t)c * N, sigma_kind));
+    for (int c = 0; c < dim; c++) RQ_TRY(timed_sigma(h, V + (size_t)c * N, HV + (size_t)c * N, sigma_kind));
     out.n_sigma += dim;
     std::vector<double> P((size_t)KMAX * KMAX, 0.0);
     auto proj_cols = [&](int c0, int c1, int m) -> int {  // P[i][c] for i < m, c in [c0, c1)
@@ -423,7 +440,7 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
             }
             if (redundant) { out.converged = true; out.reason = 2; break; }
             for (int c = 0; c < nr; c++)
-                RQ_TRY(sigma_device(h, V + (size_t)(dim + c) * N, HV + (size_t)(dim + c) * N, sigma_kind));
+                RQ_TRY(timed_sigma(h, V + (size_t)(dim + c) * N, HV + (size_t)(dim + c) * N, sigma_kind));
             out.n_sigma += nr;
             RQ_TRY(proj_cols(dim, dim + nr, dim + nr));
             dim += nr;
@@ -448,13 +465,14 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
 int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double tol, double etol, int max_iter,
                   int mode, int precond, double* evals, double* evecs, risqgpu_dstats* st) {
     auto t0 = std::chrono::steady_clock::now();
+    h->sigma_ms_acc = 0.0;
     if (!h->built) { h->err = "davidson before build"; return RISQGPU_ERR_INVALID; }
     if (nroots < 1 || nroots > RMAX) { h->err = "nroots must be in [1, 8]"; return RISQGPU_ERR_INVALID; }
     if ((size_t)nroots > h->N) { h->err = "nroots > N"; return RISQGPU_ERR_INVALID; }
     if (init && (ninit < 1 || ninit > nroots + 10)) { h->err = "bad ninit"; return RISQGPU_ERR_INVALID; }
     if (init && nroots > 1 && ninit < nroots) { h->err = "ninit must be >= nroots for several roots"; return RISQGPU_ERR_INVALID; }
-    if (mode == RISQGPU_MODE_MIXED && h->precision != RISQGPU_MIXED) {
-        h->err = "MIXED mode needs a MIXED build (FP32 values + FP32 remainder)";
+    if (mode == RISQGPU_MODE_MIXED && h->precision == RISQGPU_FP64) {
+        h->err = "MIXED mode needs a MIXED (or FP32) build";
         return RISQGPU_ERR_INVALID;
     }
     if (mode == RISQGPU_MODE_FP64 && h->precision == RISQGPU_FP32) {
@@ -498,7 +516,8 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         RQ_TRY(davidson_loop<float>(wk, nroots, init_int, use_init, false, nullptr, tol, etol, max_iter, 1, fscale, ritz, hr,
                                     lo));
         const int n32 = lo.n_sigma;
-        if (lo.converged) {
+        // closing FP64 sweeps need the FP32 remainder; an FP32-only build stops here
+        if (lo.converged && h->precision == RISQGPU_MIXED) {
             // closing FP64-sigma sweeps from the FP64 Ritz vectors
             LoopOut lr;
             double *seed = nullptr;
@@ -535,6 +554,7 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         st->learned_fallbacks = lo.fallbacks;
         for (int c = 0; c < nroots && c < 8; c++) st->residual[c] = lo.res[c];
         st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        st->ms_sigma = h->sigma_ms_acc;
     }
     return lo.converged ? RISQGPU_OK : RISQGPU_ERR_NOT_CONVERGED;
 }

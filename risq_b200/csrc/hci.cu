@@ -8,6 +8,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -220,6 +222,12 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
     free_dets(h);
     RQ_TRY(set_dets_impl(h, h->wf_dets.data(), 1, 0, h->wf_diag.data()));
     size_t n_stored = 0;
+    const bool verbose = std::getenv("RISQGPU_VERBOSE") != nullptr;
+    // precision -1: FP64 while the matrix fits in device memory, then FP32 values with
+    // an FP32 Davidson (coefficients for selection only need FP32 accuracy)
+    const bool auto_prec = precision < 0;
+    int cur_prec = auto_prec ? RISQGPU_FP64 : precision;
+    int cur_mode = auto_prec ? RISQGPU_MODE_FP64 : mode;
     for (int iter = 1; iter <= max_iter; iter++) {
         risqgpu_var_iter rec;
         std::memset(&rec, 0, sizeof(rec));
@@ -243,7 +251,23 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
         const size_t N = h->wf_diag.size();
         if (!(h->built && added == 0)) {
             RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, n_stored, h->wf_diag.data()));
-            RQ_TRY(build_h_impl(h, precision, RISQGPU_BUILDER_AUTO, nullptr));
+            int rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
+            if (rc == RISQGPU_ERR_OOM && n_stored > 0) {
+                // no room for the kept previous matrix next to the new one: rebuild every pair
+                // (the stored set then differs from the reference's history only by singles of
+                // magnitude <= 1e-12 that a legacy-rule build (N <= 100) had kept)
+                if (verbose) std::fprintf(stderr, "[risqgpu] iter %d: incremental build does not fit, rebuilding\n", iter);
+                RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, 0, h->wf_diag.data()));
+                rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
+            }
+            if (rc == RISQGPU_ERR_OOM && auto_prec && cur_prec == RISQGPU_FP64) {
+                if (verbose) std::fprintf(stderr, "[risqgpu] iter %d: FP64 matrix does not fit, FP32 from here\n", iter);
+                cur_prec = RISQGPU_FP32;
+                cur_mode = RISQGPU_MODE_MIXED;
+                RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, 0, h->wf_diag.data()));
+                rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
+            }
+            RQ_TRY(rc);
             n_stored = N;
         }
         auto t2 = clk::now();
@@ -252,7 +276,7 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
         risqgpu_dstats ds;
         std::memset(&ds, 0, sizeof(ds));
         int rc = davidson_impl(h, 1, iter > 1 ? h->wf_coeffs.data() : nullptr, iter > 1 ? 1 : 0, 1e-4, 1e-8,
-                               dav_max_iter, mode, precond, &e, vec.data(), &ds);
+                               dav_max_iter, cur_mode, precond, &e, vec.data(), &ds);
         if (rc == RISQGPU_OK) {
             h->wf_energy = e;
             h->wf_coeffs = vec;
@@ -268,6 +292,13 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
         rec.ms_build = std::chrono::duration<double, std::milli>(t2 - t1).count();
         rec.ms_davidson = std::chrono::duration<double, std::milli>(t3 - t2).count();
         h->var_log.push_back(rec);
+        if (verbose)
+            std::fprintf(stderr,
+                         "[risqgpu] iter %d eps %.3g N %llu new %llu nnz_upper %llu E %.10f dav %d%s "
+                         "sel %.1f ms build %.1f ms dav %.1f ms\n",
+                         iter, eps, (unsigned long long)N, (unsigned long long)added,
+                         (unsigned long long)h->nnz_upper, h->wf_energy, ds.iters, rc == RISQGPU_OK ? "" : " (not converged)",
+                         rec.ms_select, rec.ms_build, rec.ms_davidson);
         eps_iter.next();  // src/var/mod.rs:123
     }
     if (energy) *energy = h->wf_energy;

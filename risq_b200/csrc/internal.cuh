@@ -39,7 +39,10 @@ struct MlpWeights {
 
 struct risqgpu {
     int device = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;        // stream all work is issued on
+    cudaStream_t own_stream = nullptr;    // the handle's own stream
+    double sigma_ms_acc = 0.0;            // event time of sigma launches inside Davidson
+    bool time_sigma = false;
     std::string err;
 
     // integrals (reference packed layout)

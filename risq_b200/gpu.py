@@ -195,7 +195,11 @@ class GpuHam:
         self.n = N
         return e.value, d, c, g, [recs[i].as_dict() for i in range(k.value)]
 
-    def sparse_optimize(self, init_coeffs=None, coeff_eps=1e-4, energy_eps=1e-8, precision=A.FP64,
+    def set_stream(self, stream_ptr):
+        """Issue the handle's work on a caller cudaStream_t (int address); None = own stream."""
+        A.check(A.lib().risqgpu_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None), self._h)
+
+    def sparse_optimize(self, init_coeffs=None, coeff_eps=1e-4, energy_eps=1e-8, max_iter=50, precision=A.FP64,
                         mode=A.MODE_FP64, precond=A.PRECOND_DPR):
         """Build (or extend) H for the current set and run Davidson for the ground state.
 
@@ -209,6 +213,7 @@ class GpuHam:
         if init_coeffs is not None:
             init_coeffs = np.ascontiguousarray(init_coeffs, dtype=np.float64)
             ip = A.ptr(init_coeffs, A._dp)
-        A.check(A.lib().risqgpu_sparse_optimize(self._h, ip, coeff_eps, energy_eps, precision, mode, precond,
-                                                C.byref(e), A.ptr(c, A._dp), C.byref(hs), C.byref(ds)), self._h)
+        A.check(A.lib().risqgpu_sparse_optimize(self._h, ip, coeff_eps, energy_eps, max_iter, precision, mode,
+                                                precond, C.byref(e), A.ptr(c, A._dp), C.byref(hs), C.byref(ds)),
+                self._h)
         return e.value, c, hs.as_dict(), ds.as_dict()
