@@ -211,6 +211,23 @@ RISQGPU_API int risqgpu_variational(risqgpu_t* h, int nup, int ndn, int ncore, i
 RISQGPU_API int risqgpu_get_wf(risqgpu_t* h, uint64_t* dets, double* coeffs, double* diag, size_t cap);
 RISQGPU_API int risqgpu_var_log(risqgpu_t* h, risqgpu_var_iter* out, int cap, int* n);
 
+/* y = H x like risqgpu_sigma, but the call allocates no device memory.  This entry
+ * point has no counterpart in the reference.  It is for callers that cannot let a
+ * library allocate device memory during a solve: a host code whose pool allocator
+ * owns the device memory budget, or a Davidson loop that overlaps work on several
+ * streams, where the cudaMalloc/cudaFree pair inside risqgpu_sigma would add a
+ * device-wide synchronisation to every iteration.  x_dev and y_dev are device
+ * pointers to N doubles in the caller's determinant order (allocated by the
+ * caller); the two internal-order copies live in one static device array of 2 x
+ * 2^20 doubles (16 MiB), held by every GPU that loads the library until the
+ * process exits, so sets of more than 1,048,576 determinants are rejected with
+ * RISQGPU_ERR_CAPACITY.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress, with the handle's device current); make that
+ * first call before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU (other handles or threads, other streams) race; the contents
+ * left by a previous call are never read.  Synchronous at return, like the others. */
+RISQGPU_API int risqgpu_sigma_noalloc(risqgpu_t* h, const double* x_dev, double* y_dev);
+
 /* Element-level entry points (parity tests): H_ii and H_ij of dets[k] / (d1[k], d2[k]). */
 RISQGPU_API int risqgpu_ham_diag(risqgpu_t* h, const uint64_t* dets, size_t n, double* out);
 RISQGPU_API int risqgpu_ham_off_diag(risqgpu_t* h, const uint64_t* d1, const uint64_t* d2, size_t n, double* out);

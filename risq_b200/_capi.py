@@ -87,6 +87,7 @@ SIGNATURES = [
     ("risqgpu_sparse_optimize", C.c_int, [_handle, _dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                           _dp, _dp, C.POINTER(HStats), C.POINTER(DStats)]),
     ("risqgpu_set_stream", C.c_int, [_handle, C.c_void_p]),
+    ("risqgpu_sigma_noalloc", C.c_int, [_handle, C.c_void_p, C.c_void_p]),
     ("risqgpu_ham_diag", C.c_int, [_handle, _u64p, C.c_size_t, _dp]),
     ("risqgpu_ham_off_diag", C.c_int, [_handle, _u64p, _u64p, C.c_size_t, _dp]),
     ("risqgpu_set_precond_mlp", C.c_int, [_handle, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _fp, _fp]),

@@ -132,6 +132,11 @@ class GpuHam:
         A.check(A.lib().risqgpu_sigma(self._h, A.ptr(Xc, A._dp), A.ptr(Y, A._dp), Xc.shape[0]), self._h)
         return Y.T.copy()
 
+    def sigma_noalloc(self, x_ptr: int, y_ptr: int):
+        """y = H x on caller-owned device buffers (caller order) with no allocation in the call
+        (at most 2^20 determinants; see risqgpu_sigma_noalloc in include/risqgpu.h)."""
+        A.check(A.lib().risqgpu_sigma_noalloc(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr)), self._h)
+
     def sigma_device(self, x_ptr: int, y_ptr: int, dtype: int = 0):
         A.check(A.lib().risqgpu_sigma_device(self._h, C.c_void_p(x_ptr), C.c_void_p(y_ptr), dtype), self._h)
 
