@@ -229,11 +229,20 @@ def main():
 
     # ---- device-resident time-to-E_var (FP64 build + plain DPR Davidson) ----
     g.set_dets(dets, 0, diag)
+    # FP64 values when they fit, else columns only with the FP64 elements recomputed in sigma
+    prec64 = _capi.FP64
+    try:
+        g.build(_capi.FP64)
+    except _capi.RisqGpuError as e:
+        if e.code != _capi.ERR_OOM:
+            raise
+        prec64 = _capi.COLS
+        say("# FP64 values do not fit one GPU: plain FP64 path recomputes elements in sigma")
     energies, builds, davs = [], [], []
     clocks = ClockSampler(local)
     clocks.start()
     for i in range(args.warmup):
-        g.build(_capi.FP64)
+        g.build(prec64)
         g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
     torch.cuda.synchronize()
     barrier()
@@ -241,7 +250,7 @@ def main():
     t_start, t_end = ev(), ev()
     t_start.record(stream)
     for i in range(args.steps):
-        hs = g.build(_capi.FP64)
+        hs = g.build(prec64)
         r = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
         energies.append(float(r.eigenvalues[0]))
         builds.append(hs)
@@ -271,7 +280,7 @@ def main():
         a, b = ev(), ev()
         a.record(stream)
         g.set_dets(dets_pinned, 0, pin_diag.numpy())
-        e_api, c_api, _, _ = g.sparse_optimize(None, 1e-4, 1e-8, max_iter=DAV_MAX_ITER)
+        e_api, c_api, _, _ = g.sparse_optimize(None, 1e-4, 1e-8, max_iter=DAV_MAX_ITER, precision=prec64)
         b.record(stream)
         torch.cuda.synchronize()
         e2e_ms.append(a.elapsed_time(b))
@@ -281,8 +290,8 @@ def main():
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e = float(et.item())
 
-    # ---- sigma roofline (FP64 CSR; x, y in the library's internal order) ----
-    g.build(_capi.FP64)
+    # ---- sigma roofline (x, y in the library's internal order) ----
+    g.build(prec64)
     nnz_u, nnz_f = g.nnz()
     x = torch.randn(N, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
@@ -297,16 +306,20 @@ def main():
     b.record(stream)
     torch.cuda.synchronize()
     t_sig = a.elapsed_time(b) / R
-    # algorithmic bytes: values + int32 columns, per row int64 start + int32 length,
-    # x and diag read once, y written once
-    b_sig = nnz_f * (8 + 4) + N * (8 + 4) + 3 * N * 8
+    # algorithmic bytes: values (none when recomputed) + int32 columns, per row int64
+    # start + int32 length, x and diag read once, y written once; the recomputing
+    # kernel also reads both strings of every determinant once (N * 16 B)
+    if prec64 == _capi.FP64:
+        b_sig = nnz_f * (8 + 4) + N * (8 + 4) + 3 * N * 8
+    else:
+        b_sig = nnz_f * 4 + N * (8 + 4) + 3 * N * 8 + N * 16
     peak, peak_kind = peaks()
     sig_gbs = b_sig / (t_sig * 1e-3) / 1e9
 
     # ---- mixed precision (FP32 sigma, FP64 dots / RR, closing FP64 sweeps) ----
     a, b = ev(), ev()
     a.record(stream)
-    hs_m = g.build(_capi.MIXED)
+    hs_m = g.build(_capi.FP32)
     rm = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=_capi.MODE_MIXED)
     b.record(stream)
     torch.cuda.synchronize()
@@ -340,10 +353,12 @@ def main():
         "config": {"workload": f"hci n{cfg['n']} {cfg['nel']}a{cfg['nel']}b eps_var {cfg['eps']:g} seed 0",
                    "n_dets": int(N), "nnz_upper": int(nnz_u), "nnz_full": int(nnz_f),
                    "step": "FP64 sparse-H build + plain DPR Davidson to E_var (tol 1e-4, etol 1e-8)",
+                   "fp64_storage": "values" if prec64 == _capi.FP64 else "columns, elements recomputed in sigma",
                    "l2": "CSR stream larger than L2 every step", "parallelism": f"replicas x{world}"},
         "e2e": {"value": N * world / (e2e * 1e-3), "unit": "dets/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": int(N * 40), "d2h_bytes_per_step": int(N * 8 + 8)},
-        "roofline": {"bound": "hbm", "kernel": "k_spmv<FP64>", "achieved": sig_gbs, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": "k_spmv<FP64>" if prec64 == _capi.FP64 else "k_spmv_otf",
+                     "achieved": sig_gbs, "peak": peak, "unit": "GB/s",
                      "frac": sig_gbs / peak, "peak_kind": peak_kind, "traffic": None,
                      "bytes_per_launch": int(b_sig), "ms_per_launch": t_sig},
         "time_to_evar_ms": {"fp64_plain": ms_max, "mixed_dpr": ms_mixed,

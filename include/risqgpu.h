@@ -63,7 +63,9 @@ enum risqgpu_status {
 enum risqgpu_precision {
     RISQGPU_FP64 = 0,   /* FP64 values, int32 columns */
     RISQGPU_FP32 = 1,   /* FP32 values (rounded from FP64 Slater-Condon), int32 columns */
-    RISQGPU_MIXED = 2   /* FP32 values plus an FP32 remainder, so both FP32 and ~FP64 sigma run */
+    RISQGPU_MIXED = 2,  /* FP32 values plus an FP32 remainder, so both FP32 and ~FP64 sigma run */
+    RISQGPU_COLS = 3    /* int32 columns only: the FP64 sigma recomputes every element on the fly
+                           (bitwise the stored FP64 values) for sets whose values do not fit */
 };
 
 /* Which reference builder's rule decides the stored set (src/var/davidson.rs:55-61). */
@@ -76,8 +78,9 @@ enum risqgpu_builder {
 /* Davidson arithmetic. */
 enum risqgpu_mode {
     RISQGPU_MODE_FP64 = 0,   /* FP64 sigma, FP64 vectors */
-    RISQGPU_MODE_MIXED = 1   /* FP32 sigma and FP32 basis; FP64 dots, Gram-Schmidt and Rayleigh-Ritz;
+    RISQGPU_MODE_MIXED = 1,  /* FP32 sigma and FP32 basis; FP64 dots, Gram-Schmidt and Rayleigh-Ritz;
                                 closing FP64-sigma sweeps */
+    RISQGPU_MODE_FP32 = 2    /* the FP32 stage of MIXED alone, without the closing FP64 sweeps */
 };
 
 /* Davidson preconditioner. */
@@ -163,8 +166,9 @@ RISQGPU_API int risqgpu_export_upper(risqgpu_t* h, int64_t* rowptr, int64_t* col
 RISQGPU_API int risqgpu_sigma(risqgpu_t* h, const double* x, double* y, int nvec);
 
 /* Same on device buffers in the library's internal (sorted) order; dtype 0 =
- * FP64 vectors with the FP64 (or FP32+remainder) matrix, 1 = FP32 vectors with
- * the FP32 matrix.  Used for timing without host transfers. */
+ * FP64 vectors and FP64 elements (stored FP64, stored FP32 + remainder, or
+ * recomputed from the columns for FP32 / COLS storage), 1 = FP32 vectors with the
+ * stored FP32 values.  Used for timing without host transfers. */
 RISQGPU_API int risqgpu_sigma_device(risqgpu_t* h, const void* x_dev, void* y_dev, int dtype);
 
 /* Lowest nroots eigenpairs.  init: N x ninit column-major (caller order) or NULL

@@ -135,21 +135,36 @@ __device__ __forceinline__ uint32_t c4(uint32_t p, uint32_t q, uint32_t r, uint3
     return c2(c2(p, q), c2(r, s));
 }
 
+// Integral tables in global memory, read through the read-only cache.
 struct Ints {
     const double* __restrict__ h1;  // one_body, combine_2 layout
     const double* __restrict__ h2;  // two_body, combine_4 layout
     double nuc;
+    __device__ __forceinline__ double ld1(uint32_t k) const { return __ldg(h1 + k); }
+    __device__ __forceinline__ double ld2(uint32_t k) const { return __ldg(h2 + k); }
+};
+
+// The same tables staged in shared memory by the calling kernel.
+struct IntsShared {
+    const double* h1;
+    const double* h2;
+    double nuc;
+    __device__ __forceinline__ double ld1(uint32_t k) const { return h1[k]; }
+    __device__ __forceinline__ double ld2(uint32_t k) const { return h2[k]; }
 };
 
 // Ham::one_body (0-based p, q)          src/ham/mod.rs:65-67
-__device__ __forceinline__ double one_body(const Ints& I, int p, int q) { return __ldg(I.h1 + c2(p + 1, q + 1)); }
+template <class IT>
+__device__ __forceinline__ double one_body(const IT& I, int p, int q) { return I.ld1(c2(p + 1, q + 1)); }
 // Ham::direct(p,q,r,s) = (p r | q s)    src/ham/mod.rs:72-74
-__device__ __forceinline__ double direct(const Ints& I, int p, int q, int r, int s) {
-    return __ldg(I.h2 + c4(p + 1, r + 1, q + 1, s + 1));
+template <class IT>
+__device__ __forceinline__ double direct(const IT& I, int p, int q, int r, int s) {
+    return I.ld2(c4(p + 1, r + 1, q + 1, s + 1));
 }
 // Ham::direct_plus_exchange             src/ham/mod.rs:80-82
-__device__ __forceinline__ double dpe(const Ints& I, int p, int q, int r, int s) {
-    return __dsub_rn(__ldg(I.h2 + c4(p + 1, r + 1, q + 1, s + 1)), __ldg(I.h2 + c4(p + 1, s + 1, q + 1, r + 1)));
+template <class IT>
+__device__ __forceinline__ double dpe(const IT& I, int p, int q, int r, int s) {
+    return __dsub_rn(I.ld2(c4(p + 1, r + 1, q + 1, s + 1)), I.ld2(c4(p + 1, s + 1, q + 1, r + 1)));
 }
 
 // <d1|H|d2> for one electron of spin sigma moved: s1/s2 are the two strings of
@@ -159,8 +174,8 @@ __device__ __forceinline__ double dpe(const Ints& I, int p, int q, int r, int s)
 // exactly +0.0.  Adding +0.0 leaves every partial sum unchanged, hence the loop
 // below runs over the common orbitals only and returns the same bits.  For the
 // same reason the element is bitwise symmetric in (d1, d2).
-template <int W>
-__device__ __forceinline__ double sc_single(const Ints& I, const Bits<W>& s1, const Bits<W>& s2, const Bits<W>& opp) {
+template <int W, class IT = Ints>
+__device__ __forceinline__ double sc_single(const IT& I, const Bits<W>& s1, const Bits<W>& s2, const Bits<W>& opp) {
     int i = s1.andnot(s2).ctz();
     int j = s2.andnot(s1).ctz();
     double out = one_body(I, i, j);
@@ -181,8 +196,8 @@ __device__ __forceinline__ double sc_single(const Ints& I, const Bits<W>& s1, co
 
 // Same-spin double (ham_doub, src/ham/mod.rs:180-207): i<j removed from s1,
 // k<l added in s2, value permute_2 * [(ik|jl) - (il|jk)].
-template <int W>
-__device__ __forceinline__ double sc_double_same(const Ints& I, const Bits<W>& s1, const Bits<W>& s2) {
+template <int W, class IT = Ints>
+__device__ __forceinline__ double sc_double_same(const IT& I, const Bits<W>& s1, const Bits<W>& s2) {
     Bits<W> rem = s1.andnot(s2), add = s2.andnot(s1);
     int i0 = rem.ctz();
     rem.pop_lowest();
@@ -194,8 +209,8 @@ __device__ __forceinline__ double sc_double_same(const Ints& I, const Bits<W>& s
 }
 
 // Opposite-spin double (ham_doub, src/ham/mod.rs:208-232).
-template <int W>
-__device__ __forceinline__ double sc_double_opp(const Ints& I, const Bits<W>& a1, const Bits<W>& b1,
+template <int W, class IT = Ints>
+__device__ __forceinline__ double sc_double_opp(const IT& I, const Bits<W>& a1, const Bits<W>& b1,
                                                 const Bits<W>& a2, const Bits<W>& b2) {
     int ia = a1.andnot(a2).ctz(), aa = a2.andnot(a1).ctz();
     int ib = b1.andnot(b2).ctz(), ab = b2.andnot(b1).ctz();
@@ -204,8 +219,8 @@ __device__ __forceinline__ double sc_double_opp(const Ints& I, const Bits<W>& a1
 }
 
 // ham_diag (src/ham/mod.rs:92-124), same order of accumulation.
-template <int W>
-__device__ __forceinline__ double sc_diag(const Ints& I, const Bits<W>& up, const Bits<W>& dn) {
+template <int W, class IT = Ints>
+__device__ __forceinline__ double sc_diag(const IT& I, const Bits<W>& up, const Bits<W>& dn) {
     double d = I.nuc;
     Bits<W> t = up;
     while (!t.is_zero()) { int i = t.ctz(); t.pop_lowest(); d = __dadd_rn(d, one_body(I, i, i)); }
@@ -228,6 +243,17 @@ __device__ __forceinline__ double sc_diag(const Ints& I, const Bits<W>& up, cons
         }
     }
     return d;
+}
+
+// <p|H|q> for a stored (connected, distinct) pair: the excitation class follows from
+// the two popcounts, as in ham_off_diag_no_excite (src/ham/mod.rs:256-303).
+template <int W, class IT = Ints>
+__device__ __forceinline__ double sc_pair(const IT& I, const Bits<W>& a, const Bits<W>& b, const Bits<W>& aq,
+                                          const Bits<W>& bq) {
+    const int du = (a ^ aq).popc(), dd = (b ^ bq).popc();
+    if (du == 0) return dd == 2 ? sc_single<W, IT>(I, b, bq, a) : sc_double_same<W, IT>(I, b, bq);
+    if (dd == 0) return du == 2 ? sc_single<W, IT>(I, a, aq, b) : sc_double_same<W, IT>(I, a, aq);
+    return sc_double_opp<W, IT>(I, a, b, aq, bq);
 }
 
 }  // namespace risq

@@ -218,7 +218,7 @@ struct SetView {
 };
 
 // MODE 0: count structural candidates per row.  MODE 1/2/3: evaluate and store
-// FP64 / FP32 / FP32 + FP32 remainder.
+// FP64 / FP32 / FP32 + FP32 remainder.  MODE 4: evaluate, store the columns only.
 template <int W, int MODE>
 __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double thr_single, int* __restrict__ row_counter,
                                                     int64_t* __restrict__ cnt, const int64_t* __restrict__ row_start,
@@ -267,6 +267,7 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
                     if (MODE == 1) v64[pos] = v.prev_v64[ps + t];
                     if (MODE == 2) v32[pos] = v.prev_v32[ps + t];
                     if (MODE == 3) { v32[pos] = v.prev_v32[ps + t]; vlo[pos] = v.prev_vlo[ps + t]; }
+                    // MODE 4 keeps columns only
                 }
             }
             count += pl;
@@ -369,6 +370,27 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
         if (lane == 0) {
             if (MODE == 0) cnt[p] = count;
             else row_len[p] = count;
+        }
+    }
+}
+
+// FP64 values of the stored elements (export of a columns-only build).
+template <int W>
+__global__ void k_stored_values(const uint64_t* __restrict__ up, const uint64_t* __restrict__ dn, int64_t n,
+                                const int64_t* __restrict__ row_start, const int32_t* __restrict__ row_len,
+                                const int32_t* __restrict__ cols, Ints I, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t p = warp; p < n; p += nwarps) {
+        Bits<W> a, b;
+        for (int k = 0; k < W; k++) { a.w[k] = up[k * n + p]; b.w[k] = dn[k * n + p]; }
+        for (int k = lane; k < row_len[p]; k += 32) {
+            const int64_t e = row_start[p] + k;
+            const int q = cols[e];
+            Bits<W> aq, bq;
+            for (int w = 0; w < W; w++) { aq.w[w] = up[w * n + q]; bq.w[w] = dn[w * n + q]; }
+            out[e] = sc_pair<W>(I, a, b, aq, bq);
         }
     }
 }
@@ -683,7 +705,7 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     auto t1 = clk::now();
     {
         // refuse up front when the rows cannot be stored, leaving the handle unchanged
-        size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : 8);
+        size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : (precision == RISQGPU_COLS ? 0 : 8));
         size_t need = (size_t)cap * (4 + vb) + ((size_t)64 << 20);
         size_t fr = 0, tot = 0;
         RQ_CUDA(h, cudaMemGetInfo(&fr, &tot));
@@ -702,7 +724,7 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     dfree(h->d_val32);
     dfree(h->d_val_lo);
     if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, cap));
-    else RQ_TRY(dalloc(h, h->d_val32, cap));
+    else if (precision != RISQGPU_COLS) RQ_TRY(dalloc(h, h->d_val32, cap));
     if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, cap));
     RQ_TRY(sync(h, "alloc"));
     auto t2 = clk::now();
@@ -714,9 +736,12 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     else if (precision == RISQGPU_FP32)
         k_build_rows<W, 2><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
                                                               h->d_cols, nullptr, h->d_val32, nullptr);
-    else
+    else if (precision == RISQGPU_MIXED)
         k_build_rows<W, 3><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
                                                               h->d_cols, nullptr, h->d_val32, h->d_val_lo);
+    else
+        k_build_rows<W, 4><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
+                                                              h->d_cols, nullptr, nullptr, nullptr);
     RQ_CUDA(h, cudaEventRecord(ev[3], h->stream));
     RQ_TRY(check_launch(h, "fill rows"));
     // stored count
@@ -752,7 +777,7 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
         st->candidates = (uint64_t)cap;
         st->ms_count = std::chrono::duration<double, std::milli>(t1 - t0).count();
         st->ms_fill = std::chrono::duration<double, std::milli>(t3 - t2).count();
-        size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : 8);
+        size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : (precision == RISQGPU_COLS ? 0 : 8));
         st->bytes_csr = (uint64_t)nnz * (4 + vb);
     }
     return RISQGPU_OK;
@@ -860,7 +885,7 @@ int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const 
 }
 
 int build_h_impl(risqgpu* h, int precision, int builder, risqgpu_hstats* st) {
-    if (precision < 0 || precision > 2) { h->err = "bad precision"; return RISQGPU_ERR_INVALID; }
+    if (precision < 0 || precision > 3) { h->err = "bad precision"; return RISQGPU_ERR_INVALID; }
     if (builder < 0 || builder > 2) { h->err = "bad builder"; return RISQGPU_ERR_INVALID; }
     if (h->N == 0) { h->err = "no determinants set"; return RISQGPU_ERR_INVALID; }
     if (h->nsh > 0 && h->prev_precision != precision) {
@@ -898,6 +923,20 @@ int export_upper_impl(risqgpu* h, int64_t* rowptr, int64_t* cols, double* vals, 
     RQ_CUDA(h, cudaMemcpy(orig.data(), h->d_orig, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
     if (h->precision == RISQGPU_FP64) {
         RQ_CUDA(h, cudaMemcpy(v.data(), h->d_val64, sizeof(double) * h->cap, cudaMemcpyDeviceToHost));
+    } else if (h->precision == RISQGPU_COLS) {
+        double* dv = nullptr;
+        RQ_TRY(dalloc(h, dv, h->cap));
+        Ints I{h->d_h1, h->d_h2, h->nuc};
+        if (h->W == 1)
+            k_stored_values<1><<<grid_for(h, (int64_t)n * 32), 256, 0, h->stream>>>(h->d_up, h->d_dn, (int64_t)n,
+                h->d_row_start, h->d_row_len, h->d_cols, I, dv);
+        else
+            k_stored_values<2><<<grid_for(h, (int64_t)n * 32), 256, 0, h->stream>>>(h->d_up, h->d_dn, (int64_t)n,
+                h->d_row_start, h->d_row_len, h->d_cols, I, dv);
+        RQ_TRY(check_launch(h, "stored values"));
+        RQ_TRY(sync(h, "stored values"));
+        RQ_CUDA(h, cudaMemcpy(v.data(), dv, sizeof(double) * h->cap, cudaMemcpyDeviceToHost));
+        dfree(dv);
     } else {
         std::vector<float> hi(h->cap), lo;
         RQ_CUDA(h, cudaMemcpy(hi.data(), h->d_val32, sizeof(float) * h->cap, cudaMemcpyDeviceToHost));

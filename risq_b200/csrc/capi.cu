@@ -139,7 +139,7 @@ int risqgpu_sigma_device(risqgpu_t* h, const void* x_dev, void* y_dev, int dtype
 
 int risqgpu_davidson(risqgpu_t* h, int nroots, const double* init, int ninit, double tol, double etol, int max_iter,
                      int mode, int precond, double* evals, double* evecs, risqgpu_dstats* stats) {
-    if (!h || !evals || max_iter < 1 || (mode != 0 && mode != 1) || (precond != 0 && precond != 1))
+    if (!h || !evals || max_iter < 1 || mode < 0 || mode > 2 || (precond != 0 && precond != 1))
         return RISQGPU_ERR_INVALID;
     DeviceGuard g(h->device);
     if (stats) std::memset(stats, 0, sizeof(*stats));

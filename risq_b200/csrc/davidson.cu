@@ -471,12 +471,8 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
     if ((size_t)nroots > h->N) { h->err = "nroots > N"; return RISQGPU_ERR_INVALID; }
     if (init && (ninit < 1 || ninit > nroots + 10)) { h->err = "bad ninit"; return RISQGPU_ERR_INVALID; }
     if (init && nroots > 1 && ninit < nroots) { h->err = "ninit must be >= nroots for several roots"; return RISQGPU_ERR_INVALID; }
-    if (mode == RISQGPU_MODE_MIXED && h->precision == RISQGPU_FP64) {
-        h->err = "MIXED mode needs a MIXED (or FP32) build";
-        return RISQGPU_ERR_INVALID;
-    }
-    if (mode == RISQGPU_MODE_FP64 && h->precision == RISQGPU_FP32) {
-        h->err = "FP64 mode needs an FP64 or MIXED build";
+    if (mode != RISQGPU_MODE_FP64 && (h->precision == RISQGPU_FP64 || h->precision == RISQGPU_COLS)) {
+        h->err = "the FP32 sigma of MIXED / FP32 mode needs an FP32 or MIXED build";
         return RISQGPU_ERR_INVALID;
     }
     if (precond == RISQGPU_PRECOND_LEARNED && !h->mlp.loaded) {
@@ -516,8 +512,9 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         RQ_TRY(davidson_loop<float>(wk, nroots, init_int, use_init, false, nullptr, tol, etol, max_iter, 1, fscale, ritz, hr,
                                     lo));
         const int n32 = lo.n_sigma;
-        // closing FP64 sweeps need the FP32 remainder; an FP32-only build stops here
-        if (lo.converged && h->precision == RISQGPU_MIXED) {
+        // closing FP64-sigma sweeps (stored FP32 + remainder, or elements recomputed in FP64);
+        // FP32 mode stops after the FP32 stage
+        if (lo.converged && mode == RISQGPU_MODE_MIXED) {
             // closing FP64-sigma sweeps from the FP64 Ritz vectors
             LoopOut lr;
             double *seed = nullptr;

@@ -223,8 +223,8 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
     RQ_TRY(set_dets_impl(h, h->wf_dets.data(), 1, 0, h->wf_diag.data()));
     size_t n_stored = 0;
     const bool verbose = std::getenv("RISQGPU_VERBOSE") != nullptr;
-    // precision -1: FP64 while the matrix fits in device memory, then FP32 values with
-    // an FP32 Davidson (coefficients for selection only need FP32 accuracy)
+    // precision -1: FP64 values while they fit in device memory, then columns only with
+    // the FP64 elements recomputed in sigma (FP64 arithmetic throughout)
     const bool auto_prec = precision < 0;
     int cur_prec = auto_prec ? RISQGPU_FP64 : precision;
     int cur_mode = auto_prec ? RISQGPU_MODE_FP64 : mode;
@@ -261,9 +261,10 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
                 rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
             }
             if (rc == RISQGPU_ERR_OOM && auto_prec && cur_prec == RISQGPU_FP64) {
-                if (verbose) std::fprintf(stderr, "[risqgpu] iter %d: FP64 matrix does not fit, FP32 from here\n", iter);
-                cur_prec = RISQGPU_FP32;
-                cur_mode = RISQGPU_MODE_MIXED;
+                // FP64 values do not fit: keep the columns only and recompute the FP64
+                // elements inside sigma (the same values, a quarter of the storage)
+                if (verbose) std::fprintf(stderr, "[risqgpu] iter %d: FP64 values do not fit, columns only from here\n", iter);
+                cur_prec = RISQGPU_COLS;
                 RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, 0, h->wf_diag.data()));
                 rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
             }

@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <type_traits>
 
+#include "bits.cuh"
 #include "internal.cuh"
 
 namespace risq {
@@ -75,6 +76,73 @@ __global__ void __launch_bounds__(256) k_spmv(int64_t N, const int64_t* __restri
     }
 }
 
+// FP64 sigma that recomputes every stored element from the two determinants and
+// the integrals (Slater-Condon in FP64, bitwise the values a FP64 build stores),
+// reading only the int32 column stream from HBM.  SMEM: the packed integral tables
+// are staged in shared memory (n <= 20 fits in 227 KB).
+template <int W, bool SMEM>
+__global__ void __launch_bounds__(1024, 1) k_spmv_otf(int64_t N, const uint64_t* __restrict__ up,
+                                                      const uint64_t* __restrict__ dn,
+                                                      const int64_t* __restrict__ row_start,
+                                                      const int32_t* __restrict__ row_len,
+                                                      const int32_t* __restrict__ cols,
+                                                      const double* __restrict__ diag, Ints Ig, uint32_t n1,
+                                                      uint32_t n2, const double* __restrict__ x,
+                                                      double* __restrict__ y) {
+    extern __shared__ double sm[];
+    if constexpr (SMEM) {
+        for (uint32_t k = threadIdx.x; k < n1; k += blockDim.x) sm[k] = Ig.h1[k];
+        for (uint32_t k = threadIdx.x; k < n2; k += blockDim.x) sm[n1 + k] = Ig.h2[k];
+        __syncthreads();
+    }
+    const IntsShared Is{sm, sm + n1, Ig.nuc};
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t p = warp; p < N; p += nwarps) {
+        Bits<W> a, b;
+#pragma unroll
+        for (int k = 0; k < W; k++) { a.w[k] = __ldg(up + k * N + p); b.w[k] = __ldg(dn + k * N + p); }
+        const int64_t s = row_start[p];
+        const int len = row_len[p];
+        double acc = 0.0;
+        for (int k = lane; k < len; k += 32) {
+            const int q = __ldcs(cols + s + k);
+            Bits<W> aq, bq;
+#pragma unroll
+            for (int w = 0; w < W; w++) { aq.w[w] = __ldg(up + w * N + q); bq.w[w] = __ldg(dn + w * N + q); }
+            double v;
+            if constexpr (SMEM) v = sc_pair<W, IntsShared>(Is, a, b, aq, bq);
+            else v = sc_pair<W, Ints>(Ig, a, b, aq, bq);
+            acc += v * __ldg(x + q);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) y[p] = diag[p] * x[p] + acc;
+    }
+}
+
+template <int W>
+int launch_otf(risqgpu* h, const double* x, double* y) {
+    const int64_t n = (int64_t)h->N;
+    Ints I{h->d_h1, h->d_h2, h->nuc};
+    const size_t smem = sizeof(double) * (h->n1 + h->n2);
+    int max_smem = 0;
+    cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
+    if (smem <= (size_t)max_smem) {
+        RQ_CUDA(h, cudaFuncSetAttribute(k_spmv_otf<W, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_spmv_otf<W, true><<<num_sms(h), 1024, smem, h->stream>>>(n, h->d_up, h->d_dn, h->d_row_start, h->d_row_len,
+                                                                   h->d_cols, h->d_diag, I, (uint32_t)h->n1,
+                                                                   (uint32_t)h->n2, x, y);
+    } else {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_spmv_otf<W, false>, 1024, 0);
+        k_spmv_otf<W, false><<<num_sms(h) * std::max(occ, 1), 1024, 0, h->stream>>>(
+            n, h->d_up, h->d_dn, h->d_row_start, h->d_row_len, h->d_cols, h->d_diag, I, (uint32_t)h->n1,
+            (uint32_t)h->n2, x, y);
+    }
+    return check_launch(h, "sigma otf");
+}
+
 __global__ void k_permute_in(const double* __restrict__ x, const int32_t* __restrict__ orig, int64_t n,
                              double* __restrict__ xi) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
@@ -112,11 +180,13 @@ int sigma_device(risqgpu* h, const void* x, void* y, int kind) {
         else if (h->precision == RISQGPU_MIXED)
             k_spmv<2, double><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr,
                                                            h->d_val32, h->d_val_lo, h->d_diag, xd, yd);
-        else
-            k_spmv<3, double><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr,
-                                                           h->d_val32, nullptr, h->d_diag, xd, yd);
+        else  // FP32 or columns-only storage: exact FP64 elements recomputed on the fly
+            return h->W == 1 ? launch_otf<1>(h, xd, yd) : launch_otf<2>(h, xd, yd);
     } else {
-        if (h->precision == RISQGPU_FP64) { h->err = "FP32 sigma needs an FP32 or MIXED build"; return RISQGPU_ERR_INVALID; }
+        if (h->precision == RISQGPU_FP64 || h->precision == RISQGPU_COLS) {
+            h->err = "FP32 sigma needs an FP32 or MIXED build";
+            return RISQGPU_ERR_INVALID;
+        }
         k_spmv<1, float><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr, h->d_val32,
                                                       nullptr, h->d_diag, (const float*)x, (float*)y);
     }

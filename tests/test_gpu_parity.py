@@ -215,3 +215,34 @@ def test_invalid_inputs_are_rejected():
             g.davidson(1, mode=_capi.MODE_MIXED)  # FP64 storage cannot run the FP32 sigma
         with pytest.raises(_capi.RisqGpuError):
             g.set_dets(dets[:5], 3, diag[:5])  # n_stored_h must equal the previous size
+
+
+@pytest.mark.parametrize("name", ["be2", "f2"])
+def test_columns_only_build_and_recomputed_sigma(name):
+    """COLS storage keeps the columns; sigma recomputes the FP64 elements, which are
+    bitwise the stored ones, so export and sigma match the FP64 build."""
+    ints, p = H.golden_system(name)
+    _, dets, coeffs, diag, _ = H.oracle_hci(name)
+    rng = np.random.default_rng(5)
+    x = rng.standard_normal(len(dets))
+    with _gpu(ints) as g:
+        g.set_dets(dets, 0, diag)
+        g.build(_capi.FP64)
+        ref_csr = g.export_upper()
+        ref_y = g.matrix_vector_prod(x)
+        r64 = g.davidson(1, None, 1e-4, 1e-8, 50)
+        g.build(_capi.COLS)
+        csr = g.export_upper()
+        for a, b in zip(csr, ref_csr):
+            np.testing.assert_array_equal(a, b)
+        y = g.matrix_vector_prod(x)
+        assert np.max(np.abs(y - ref_y)) <= 1e-12 * np.max(np.abs(ref_y))
+        r = g.davidson(1, None, 1e-4, 1e-8, 50)
+        assert abs(r.eigenvalues[0] - r64.eigenvalues[0]) < 1e-9
+        # FP32 storage: FP32 stage + closing sweeps with the recomputed FP64 elements
+        g.build(_capi.FP32)
+        m = g.davidson(1, None, 1e-4, 1e-8, 50, mode=_capi.MODE_MIXED)
+        assert m.converged and abs(m.eigenvalues[0] - r64.eigenvalues[0]) < 1e-6
+        assert 0 < m.stats["n_sigma_fp64"] < m.stats["n_sigma"]
+        f = g.davidson(1, None, 1e-4, 1e-8, 50, mode=_capi.MODE_FP32)
+        assert f.converged and f.stats["n_sigma_fp64"] == 0
