@@ -217,16 +217,35 @@ struct SetView {
     }
 };
 
+// Kinds of structural hits, evaluated in batches.
+enum HitKind : int { K_SING_B = 0, K_SING_A = 1, K_DOUB_B = 2, K_DOUB_A = 3, K_OPP = 4 };
+
 // MODE 0: count structural candidates per row.  MODE 1/2/3: evaluate and store
 // FP64 / FP32 / FP32 + FP32 remainder.  MODE 4: evaluate, store the columns only.
+//
+// One warp per row.  The scans visit candidates 32 at a time; only a minority are
+// connected, so evaluating Slater-Condon in place would run with a few lanes
+// active.  Connected candidates are appended instead to one of two per-warp queues
+// in shared memory (singles, which sum over the occupied orbitals, and doubles,
+// which read one or two integrals), and each queue is evaluated whenever it holds
+// 32 entries, with every lane busy.  Stored elements are written in queue order.
 template <int W, int MODE>
 __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double thr_single, int* __restrict__ row_counter,
                                                     int64_t* __restrict__ cnt, const int64_t* __restrict__ row_start,
                                                     int32_t* __restrict__ row_len, int32_t* __restrict__ cols,
                                                     double* __restrict__ v64, float* __restrict__ v32,
                                                     float* __restrict__ vlo) {
+    constexpr int WARPS = 256 / 32;
+    constexpr int QCAP = 64;  // < 32 pending + 32 new
+    __shared__ int s_q[WARPS][2][QCAP];
+    __shared__ unsigned char s_k[WARPS][2][QCAP];
     const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
+    int* const qs = s_q[wib][0];
+    int* const qd = s_q[wib][1];
+    unsigned char* const ks = s_k[wib][0];
+    unsigned char* const kd = s_k[wib][1];
     for (;;) {
         int p = 0;
         if (lane == 0) p = atomicAdd(row_counter, 1);
@@ -236,6 +255,7 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
         const bool p_new = v.nsh == 0 || v.orig[p] >= v.nsh;
         int64_t base = MODE ? row_start[p] : 0;
         int count = 0;
+        int ns = 0, nd = 0;  // queue fill, warp-uniform
 
         auto store = [&](int64_t pos, int q, double val) {
             cols[pos] = q;
@@ -247,10 +267,47 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
                 vlo[pos] = (float)(val - (double)hi);
             }
         };
-        auto emit = [&](bool ok, int q, double val) {
-            unsigned m = __ballot_sync(FULL, ok);
-            if (MODE && ok) store(base + count + __popc(m & lt), q, val);
+        // evaluate queue entries [0, take) on lanes [0, take), store the non-zero ones
+        auto flush = [&](int* qq, unsigned char* kk, int& nq, int take) {
+            bool ok = false;
+            double val = 0.0;
+            int q = -1;
+            if (lane < take) {
+                q = qq[lane];
+                const int kind = kk[lane];
+                const Bits<W> aq = v.up_at(q), bq = v.dn_at(q);
+                if (kind == K_SING_B) { val = sc_single<W>(I, b, bq, a); ok = fabs(val) > thr_single; }
+                else if (kind == K_SING_A) { val = sc_single<W>(I, a, aq, b); ok = fabs(val) > thr_single; }
+                else if (kind == K_DOUB_B) { val = sc_double_same<W>(I, b, bq); ok = val != 0.0; }
+                else if (kind == K_DOUB_A) { val = sc_double_same<W>(I, a, aq); ok = val != 0.0; }
+                else { val = sc_double_opp<W>(I, a, b, aq, bq); ok = val != 0.0; }
+            }
+            const unsigned m = __ballot_sync(FULL, ok);
+            if (ok) store(base + count + __popc(m & lt), q, val);
             count += __popc(m);
+            const int rem = nq - take;
+            int tq = 0;
+            unsigned char tk = 0;
+            if (lane < rem) { tq = qq[take + lane]; tk = kk[take + lane]; }
+            __syncwarp();
+            if (lane < rem) { qq[lane] = tq; kk[lane] = tk; }
+            __syncwarp();
+            nq = rem;
+        };
+        auto push = [&](bool hit, bool single, int q, int kind) {
+            if (MODE == 0) {
+                count += __popc(__ballot_sync(FULL, hit));
+                return;
+            }
+            const unsigned ms = __ballot_sync(FULL, hit && single);
+            const unsigned md = __ballot_sync(FULL, hit && !single);
+            if (hit && single) { const int pos = ns + __popc(ms & lt); qs[pos] = q; ks[pos] = (unsigned char)kind; }
+            if (hit && !single) { const int pos = nd + __popc(md & lt); qd[pos] = q; kd[pos] = (unsigned char)kind; }
+            ns += __popc(ms);
+            nd += __popc(md);
+            __syncwarp();
+            if (ns >= 32) flush(qs, ks, ns, 32);
+            if (nd >= 32) flush(qd, kd, nd, 32);
         };
 
         // (0) elements kept from the previous build (pairs of old determinants)
@@ -279,18 +336,13 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
             const int s = v.ga_start[g], e = v.ga_start[g + 1];
             for (int t0 = s; t0 < e; t0 += 32) {
                 const int q = t0 + lane;
-                bool ok = false;
-                double val = 0.0;
+                bool hit = false;
+                int d = 0;
                 if (q < e && q != p) {
-                    const Bits<W> bq = v.dn_at(q);
-                    const int d = (b ^ bq).popc();
-                    if (d <= 4 && (p_new || v.orig[q] >= v.nsh)) {
-                        if (MODE == 0) ok = true;
-                        else if (d == 2) { val = sc_single<W>(I, b, bq, a); ok = fabs(val) > thr_single; }
-                        else { val = sc_double_same<W>(I, b, bq); ok = val != 0.0; }
-                    }
+                    d = (b ^ v.dn_at(q)).popc();
+                    hit = d <= 4 && (p_new || v.orig[q] >= v.nsh);
                 }
-                emit(ok, q, val);
+                push(hit, d == 2, q, d == 2 ? K_SING_B : K_DOUB_B);
             }
         }
         // (2) same beta string: alpha singles and alpha-alpha doubles
@@ -299,22 +351,16 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
             const int s = v.gb_start[g], e = v.gb_start[g + 1];
             for (int t0 = s; t0 < e; t0 += 32) {
                 const int t = t0 + lane;
-                bool ok = false;
-                double val = 0.0;
-                int q = -1;
+                bool hit = false;
+                int d = 0, q = -1;
                 if (t < e) {
-                    const Bits<W> aq = v.upb_at(t);
-                    const int d = (a ^ aq).popc();
+                    d = (a ^ v.upb_at(t)).popc();
                     if (d != 0 && d <= 4) {
                         q = v.order_b[t];
-                        if (p_new || v.orig[q] >= v.nsh) {
-                            if (MODE == 0) ok = true;
-                            else if (d == 2) { val = sc_single<W>(I, a, aq, b); ok = fabs(val) > thr_single; }
-                            else { val = sc_double_same<W>(I, a, aq); ok = val != 0.0; }
-                        }
+                        hit = p_new || v.orig[q] >= v.nsh;
                     }
                 }
-                emit(ok, q, val);
+                push(hit, d == 2, q, d == 2 ? K_SING_A : K_DOUB_A);
             }
         }
         // (3) alpha single-partner groups: opposite-spin doubles
@@ -348,27 +394,24 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
                     }
                     const int gsj = __shfl_sync(FULL, gs, j);
                     const int exj = __shfl_sync(FULL, excl, j);
-                    bool ok = false;
-                    double val = 0.0;
+                    bool hit = false;
                     int q = -1;
                     if (my < total) {
                         q = gsj + (my - exj);
-                        const Bits<W> bq = v.dn_at(q);
-                        if ((b ^ bq).popc() == 2 && (p_new || v.orig[q] >= v.nsh)) {
-                            if (MODE == 0) ok = true;
-                            else {
-                                const Bits<W> aq = v.up_at(q);
-                                val = sc_double_opp<W>(I, a, b, aq, bq);
-                                ok = val != 0.0;
-                            }
-                        }
+                        hit = (b ^ v.dn_at(q)).popc() == 2 && (p_new || v.orig[q] >= v.nsh);
                     }
-                    emit(ok, q, val);
+                    push(hit, false, q, K_OPP);
                 }
             }
         }
+        if (MODE) {
+            if (ns > 0) flush(qs, ks, ns, ns);
+            if (nd > 0) flush(qd, kd, nd, nd);
+        }
         if (lane == 0) {
-            if (MODE == 0) cnt[p] = count;
+            // row capacities are rounded up to 4 elements so that every row starts on a
+            // 16-byte (columns) / 32-byte (FP64 values) boundary for vector loads
+            if (MODE == 0) cnt[p] = (count + 3) & ~3;
             else row_len[p] = count;
         }
     }
