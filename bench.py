@@ -229,15 +229,20 @@ def main():
 
     # ---- device-resident time-to-E_var (FP64 build + plain DPR Davidson) ----
     g.set_dets(dets, 0, diag)
-    # FP64 values when they fit, else columns only with the FP64 elements recomputed in sigma
-    prec64 = _capi.FP64
-    try:
-        g.build(_capi.FP64)
-    except _capi.RisqGpuError as e:
-        if e.code != _capi.ERR_OOM:
-            raise
-        prec64 = _capi.COLS
-        say("# FP64 values do not fit one GPU: plain FP64 path recomputes elements in sigma")
+    def first_fitting(precs):
+        for pr in precs:
+            try:
+                g.build(pr)
+                return pr
+            except _capi.RisqGpuError as e:
+                if e.code != _capi.ERR_OOM:
+                    raise
+                say(f"# storage {pr} does not fit one GPU")
+        raise RuntimeError("no storage mode fits")
+
+    # FP64 rows when both triangles fit; else the upper triangle (the reference's
+    # SparseMatUpperTri layout); else columns only with the elements recomputed in sigma
+    prec64 = first_fitting([_capi.FP64, _capi.FP64_UPPER, _capi.COLS])
     energies, builds, davs = [], [], []
     clocks = ClockSampler(local)
     clocks.start()
@@ -311,6 +316,8 @@ def main():
     # kernel also reads both strings of every determinant once (N * 16 B)
     if prec64 == _capi.FP64:
         b_sig = nnz_f * (8 + 4) + N * (8 + 4) + 3 * N * 8
+    elif prec64 == _capi.FP64_UPPER:  # each pair once; y is read-modify-written in L2
+        b_sig = nnz_u * (8 + 4) + N * (8 + 4) + 3 * N * 8
     else:
         b_sig = nnz_f * 4 + N * (8 + 4) + 3 * N * 8 + N * 16
     peak, peak_kind = peaks()
@@ -318,8 +325,9 @@ def main():
 
     # ---- mixed precision (FP32 sigma, FP64 dots / RR, closing FP64 sweeps) ----
     a, b = ev(), ev()
+    precm = first_fitting([_capi.MIXED, _capi.MIXED_UPPER])
     a.record(stream)
-    hs_m = g.build(_capi.FP32)
+    hs_m = g.build(precm)
     rm = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=_capi.MODE_MIXED)
     b.record(stream)
     torch.cuda.synchronize()
@@ -335,7 +343,7 @@ def main():
     b.record(stream)
     torch.cuda.synchronize()
     t_sig32 = a.elapsed_time(b) / R
-    b_sig32 = nnz_f * (4 + 4) + N * (8 + 4) + N * (4 + 4 + 8)
+    b_sig32 = (nnz_f if precm == _capi.MIXED else nnz_u) * (4 + 4) + N * (8 + 4) + N * (4 + 4 + 8)
 
     line = {
         "metric": METRIC,
@@ -353,15 +361,19 @@ def main():
         "config": {"workload": f"hci n{cfg['n']} {cfg['nel']}a{cfg['nel']}b eps_var {cfg['eps']:g} seed 0",
                    "n_dets": int(N), "nnz_upper": int(nnz_u), "nnz_full": int(nnz_f),
                    "step": "FP64 sparse-H build + plain DPR Davidson to E_var (tol 1e-4, etol 1e-8)",
-                   "fp64_storage": "values" if prec64 == _capi.FP64 else "columns, elements recomputed in sigma",
+                   "fp64_storage": {_capi.FP64: "both triangles", _capi.FP64_UPPER: "upper triangle",
+                                    _capi.COLS: "columns, elements recomputed in sigma"}[prec64],
+                   "mixed_storage": None,
                    "l2": "CSR stream larger than L2 every step", "parallelism": f"replicas x{world}"},
         "e2e": {"value": N * world / (e2e * 1e-3), "unit": "dets/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": int(N * 40), "d2h_bytes_per_step": int(N * 8 + 8)},
-        "roofline": {"bound": "hbm", "kernel": "k_spmv<FP64>" if prec64 == _capi.FP64 else "k_spmv_otf",
+        "roofline": {"bound": "hbm", "kernel": {_capi.FP64: "k_spmv<FP64>", _capi.FP64_UPPER: "k_spmv_upper<FP64>",
+                                                _capi.COLS: "k_spmv_otf"}[prec64],
                      "achieved": sig_gbs, "peak": peak, "unit": "GB/s",
                      "frac": sig_gbs / peak, "peak_kind": peak_kind, "traffic": None,
                      "bytes_per_launch": int(b_sig), "ms_per_launch": t_sig},
         "time_to_evar_ms": {"fp64_plain": ms_max, "mixed_dpr": ms_mixed,
+                            "mixed_storage": "both triangles" if precm == _capi.MIXED else "upper triangle",
                             "dE_mixed_uHa": abs(float(rm.eigenvalues[0]) - e64) * 1e6,
                             "fp64_iters": dstat["iters"], "mixed_iters": rm.stats["iters"],
                             "mixed_fp64_sigmas": rm.stats["n_sigma_fp64"]},

@@ -64,8 +64,14 @@ enum risqgpu_precision {
     RISQGPU_FP64 = 0,   /* FP64 values, int32 columns */
     RISQGPU_FP32 = 1,   /* FP32 values (rounded from FP64 Slater-Condon), int32 columns */
     RISQGPU_MIXED = 2,  /* FP32 values plus an FP32 remainder, so both FP32 and ~FP64 sigma run */
-    RISQGPU_COLS = 3    /* int32 columns only: the FP64 sigma recomputes every element on the fly
+    RISQGPU_COLS = 3,   /* int32 columns only: the FP64 sigma recomputes every element on the fly
                            (bitwise the stored FP64 values) for sets whose values do not fit */
+    /* Upper triangle only (each pair once, as the reference's SparseMatUpperTri): half the
+     * storage; sigma adds the transposed half with atomic adds into y (sums in a
+     * run-dependent order).  Built from scratch every time (no n_stored_h reuse). */
+    RISQGPU_FP64_UPPER = 4,
+    RISQGPU_FP32_UPPER = 5,
+    RISQGPU_MIXED_UPPER = 6
 };
 
 /* Which reference builder's rule decides the stored set (src/var/davidson.rs:55-61). */

@@ -20,7 +20,7 @@ ERR_NOT_CONVERGED = 4
 ERR_NO_DEVICE = 5
 ERR_CAPACITY = 6
 
-FP64, FP32, MIXED, COLS = 0, 1, 2, 3
+FP64, FP32, MIXED, COLS, FP64_UPPER, FP32_UPPER, MIXED_UPPER = 0, 1, 2, 3, 4, 5, 6
 BUILDER_AUTO, BUILDER_FAST, BUILDER_LEGACY = 0, 1, 2
 MODE_FP64, MODE_MIXED, MODE_FP32 = 0, 1, 2
 PRECOND_DPR, PRECOND_LEARNED = 0, 1

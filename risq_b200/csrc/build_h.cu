@@ -115,10 +115,11 @@ __global__ void k_segment_starts(const int32_t* __restrict__ incl, int64_t n, in
 template <int W>
 __global__ void k_beta_views(const int32_t* __restrict__ order_b, const int32_t* __restrict__ gid_t,
                              const uint64_t* __restrict__ up, int64_t n, int32_t* __restrict__ gb,
-                             uint64_t* __restrict__ up_b) {
+                             int32_t* __restrict__ pos_b, uint64_t* __restrict__ up_b) {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         int64_t p = order_b[t];
         gb[p] = gid_t[t];
+        pos_b[p] = (int32_t)t;
         for (int k = 0; k < W; k++) up_b[k * n + t] = up[k * n + p];
     }
 }
@@ -182,6 +183,7 @@ struct SetView {
     const int32_t* __restrict__ gb;
     const int32_t* __restrict__ gb_start;
     const int32_t* __restrict__ order_b;
+    const int32_t* __restrict__ pos_b;
     const int32_t* __restrict__ pa_start;
     const int32_t* __restrict__ pa_list;
     const int32_t* __restrict__ orig;
@@ -230,7 +232,8 @@ enum HitKind : int { K_SING_B = 0, K_SING_A = 1, K_DOUB_B = 2, K_DOUB_A = 3, K_O
 // which read one or two integrals), and each queue is evaluated whenever it holds
 // 32 entries, with every lane busy.  Stored elements are written in queue order.
 template <int W, int MODE>
-__global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double thr_single, int* __restrict__ row_counter,
+__global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double thr_single, int upper,
+                                                    int* __restrict__ row_counter,
                                                     int64_t* __restrict__ cnt, const int64_t* __restrict__ row_start,
                                                     int32_t* __restrict__ row_len, int32_t* __restrict__ cols,
                                                     double* __restrict__ v64, float* __restrict__ v32,
@@ -295,6 +298,7 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
             nq = rem;
         };
         auto push = [&](bool hit, bool single, int q, int kind) {
+            hit = hit && (!upper || q > p);
             if (MODE == 0) {
                 count += __popc(__ballot_sync(FULL, hit));
                 return;
@@ -331,9 +335,10 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
         }
 
         // (1) same alpha string: beta singles and beta-beta doubles
+        // (upper storage only needs q > p: the group is contiguous, start after p)
         {
             const int g = v.ga[p];
-            const int s = v.ga_start[g], e = v.ga_start[g + 1];
+            const int s = upper ? p + 1 : v.ga_start[g], e = v.ga_start[g + 1];
             for (int t0 = s; t0 < e; t0 += 32) {
                 const int q = t0 + lane;
                 bool hit = false;
@@ -346,9 +351,10 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
             }
         }
         // (2) same beta string: alpha singles and alpha-alpha doubles
+        // (a beta group lists its dets in increasing internal index: start after p's slot)
         {
             const int g = v.gb[p];
-            const int s = v.gb_start[g], e = v.gb_start[g + 1];
+            const int s = upper ? v.pos_b[p] + 1 : v.gb_start[g], e = v.gb_start[g + 1];
             for (int t0 = s; t0 < e; t0 += 32) {
                 const int t = t0 + lane;
                 bool hit = false;
@@ -373,7 +379,8 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
                 if (lane < nvalid) {
                     const int g2 = v.pa_list[c0 + lane];
                     gs = v.ga_start[g2];
-                    gl = v.ga_start[g2 + 1] - gs;
+                    // groups are ordered by index: a lower group holds only q < p
+                    gl = (upper && g2 < g) ? 0 : v.ga_start[g2 + 1] - gs;
                 }
                 int incl = gl;
 #pragma unroll
@@ -608,8 +615,10 @@ int build_groups(risqgpu* h, const uint64_t* d_aos, const double* d_diag_in) {
     RQ_TRY(dalloc(h, gid_t, n));
     RQ_TRY(segments(h, head, n, gid_t, h->d_gb_start, h->G_b));
     RQ_TRY(dalloc(h, h->d_gb, n));
+    RQ_TRY(dalloc(h, h->d_pos_b, n));
     RQ_TRY(dalloc(h, h->d_up_b, (size_t)W * n));
-    k_beta_views<W><<<grid_for(h, n), 256, 0, h->stream>>>(h->d_order_b, gid_t, h->d_up, n, h->d_gb, h->d_up_b);
+    k_beta_views<W><<<grid_for(h, n), 256, 0, h->stream>>>(h->d_order_b, gid_t, h->d_up, n, h->d_gb, h->d_pos_b,
+                                                           h->d_up_b);
     RQ_TRY(check_launch(h, "beta views"));
     dfree(dnb);
     dfree(gid_t);
@@ -685,7 +694,7 @@ SetView<W> make_view(risqgpu* h, bool with_prev, const int32_t* prev_inv_caller)
     SetView<W> v;
     v.up = h->d_up; v.dn = h->d_dn; v.up_b = h->d_up_b; v.N = (int64_t)h->N;
     v.ga = h->d_ga; v.ga_start = h->d_ga_start; v.gb = h->d_gb; v.gb_start = h->d_gb_start;
-    v.order_b = h->d_order_b; v.pa_start = h->d_pa_start; v.pa_list = h->d_pa_list;
+    v.order_b = h->d_order_b; v.pos_b = h->d_pos_b; v.pa_start = h->d_pa_start; v.pa_list = h->d_pa_list;
     v.orig = h->d_orig; v.nsh = (int64_t)h->nsh; v.inv = h->d_inv;
     v.prev_inv_of_caller = with_prev ? prev_inv_caller : nullptr;
     v.prev_row_start = h->d_prev_row_start; v.prev_row_len = h->d_prev_row_len; v.prev_cols = h->d_prev_cols;
@@ -700,7 +709,7 @@ __global__ void k_invert(const int32_t* __restrict__ orig, int64_t n, int32_t* _
 }
 
 template <int W>
-int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
+int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats* st) {
     using clk = std::chrono::steady_clock;
     const int64_t n = (int64_t)h->N;
     const bool incremental = h->nsh > 0 && h->d_prev_row_start != nullptr;
@@ -728,7 +737,7 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     auto t0 = clk::now();
     RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
     RQ_CUDA(h, cudaEventRecord(ev[0], h->stream));
-    k_build_rows<W, 0><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, cnt, nullptr, nullptr, nullptr, nullptr,
+    k_build_rows<W, 0><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, cnt, nullptr, nullptr, nullptr, nullptr,
                                                           nullptr, nullptr);
     RQ_CUDA(h, cudaEventRecord(ev[1], h->stream));
     RQ_TRY(check_launch(h, "count rows"));
@@ -774,16 +783,16 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
     RQ_CUDA(h, cudaEventRecord(ev[2], h->stream));
     if (precision == RISQGPU_FP64)
-        k_build_rows<W, 1><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
+        k_build_rows<W, 1><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start, h->d_row_len,
                                                               h->d_cols, h->d_val64, nullptr, nullptr);
     else if (precision == RISQGPU_FP32)
-        k_build_rows<W, 2><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
+        k_build_rows<W, 2><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start, h->d_row_len,
                                                               h->d_cols, nullptr, h->d_val32, nullptr);
     else if (precision == RISQGPU_MIXED)
-        k_build_rows<W, 3><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
+        k_build_rows<W, 3><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start, h->d_row_len,
                                                               h->d_cols, nullptr, h->d_val32, h->d_val_lo);
     else
-        k_build_rows<W, 4><<<blocks, threads, 0, h->stream>>>(v, I, thr, counter, nullptr, h->d_row_start, h->d_row_len,
+        k_build_rows<W, 4><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start, h->d_row_len,
                                                               h->d_cols, nullptr, nullptr, nullptr);
     RQ_CUDA(h, cudaEventRecord(ev[3], h->stream));
     RQ_TRY(check_launch(h, "fill rows"));
@@ -807,9 +816,10 @@ int build_rows(risqgpu* h, int precision, double thr, risqgpu_hstats* st) {
     dfree(counter);
     dfree(cnt);
     dfree(prev_inv);
-    h->nnz_full = (uint64_t)nnz;
-    h->nnz_upper = (uint64_t)nnz / 2;
+    h->nnz_full = upper ? 2 * (uint64_t)nnz : (uint64_t)nnz;
+    h->nnz_upper = upper ? (uint64_t)nnz : (uint64_t)nnz / 2;
     h->precision = precision;
+    h->upper = upper != 0;
     float ms_c = 0.f, ms_f = 0.f;
     cudaEventElapsedTime(&ms_c, ev[0], ev[1]);
     cudaEventElapsedTime(&ms_f, ev[2], ev[3]);
@@ -846,7 +856,7 @@ static void free_prev(risqgpu* h) {
 void free_dets(risqgpu* h) {
     dfree(h->d_up); dfree(h->d_dn); dfree(h->d_up_b); dfree(h->d_orig); dfree(h->d_inv); dfree(h->d_diag);
     dfree(h->d_ga); dfree(h->d_ga_start); dfree(h->d_gb); dfree(h->d_gb_start); dfree(h->d_order_b);
-    dfree(h->d_pa_start); dfree(h->d_pa_list);
+    dfree(h->d_pos_b); dfree(h->d_pa_start); dfree(h->d_pa_list);
     free_csr(h);
     free_prev(h);
     h->N = 0;
@@ -864,6 +874,10 @@ int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const 
     if (n >= (size_t)INT32_MAX) { h->err = "more than 2^31-1 determinants"; return RISQGPU_ERR_INVALID; }
     if (nsh > n) { h->err = "n_stored_h > n"; return RISQGPU_ERR_INVALID; }
     if (nsh > 0) {
+        if (h->upper) {
+            h->err = "an upper-triangle build cannot be extended; rebuild with n_stored_h = 0";
+            return RISQGPU_ERR_INVALID;
+        }
         if (!h->built || h->N != nsh) {
             h->err = "n_stored_h must equal the size of the previously built set";
             return RISQGPU_ERR_INVALID;
@@ -901,7 +915,7 @@ int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const 
         free_csr(h);
         dfree(h->d_up); dfree(h->d_dn); dfree(h->d_up_b); dfree(h->d_inv); dfree(h->d_diag);
         dfree(h->d_ga); dfree(h->d_ga_start); dfree(h->d_gb); dfree(h->d_gb_start); dfree(h->d_order_b);
-        dfree(h->d_pa_start); dfree(h->d_pa_list);
+        dfree(h->d_pos_b); dfree(h->d_pa_start); dfree(h->d_pa_list);
         h->N = 0;
     } else {
         free_dets(h);
@@ -928,18 +942,23 @@ int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const 
 }
 
 int build_h_impl(risqgpu* h, int precision, int builder, risqgpu_hstats* st) {
-    if (precision < 0 || precision > 3) { h->err = "bad precision"; return RISQGPU_ERR_INVALID; }
+    if (precision < 0 || precision > 6) { h->err = "bad precision"; return RISQGPU_ERR_INVALID; }
     if (builder < 0 || builder > 2) { h->err = "bad builder"; return RISQGPU_ERR_INVALID; }
     if (h->N == 0) { h->err = "no determinants set"; return RISQGPU_ERR_INVALID; }
-    if (h->nsh > 0 && h->prev_precision != precision) {
-        h->err = "an incremental build must keep the previous build's precision";
+    if (h->nsh > 0 && (h->prev_precision != precision || precision >= RISQGPU_FP64_UPPER)) {
+        h->err = "an incremental build must keep the previous build's full-row precision";
         return RISQGPU_ERR_INVALID;
     }
     bool fast = builder == RISQGPU_BUILDER_FAST || (builder == RISQGPU_BUILDER_AUTO && h->N > 100);
     double thr = fast ? 1e-12 : 0.0;
     auto t0 = std::chrono::steady_clock::now();
     free_csr(h);
-    int rc = h->W == 1 ? build_rows<1>(h, precision, thr, st) : build_rows<2>(h, precision, thr, st);
+    // upper-triangle storage modes map onto the value types with the upper flag set
+    int upper = precision >= RISQGPU_FP64_UPPER ? 1 : 0;
+    int vprec = precision == RISQGPU_FP64_UPPER ? RISQGPU_FP64
+              : precision == RISQGPU_FP32_UPPER ? RISQGPU_FP32
+              : precision == RISQGPU_MIXED_UPPER ? RISQGPU_MIXED : precision;
+    int rc = h->W == 1 ? build_rows<1>(h, vprec, upper, thr, st) : build_rows<2>(h, vprec, upper, thr, st);
     if (rc) return rc;
     h->built = true;
     if (h->nsh > 0) free_prev(h);
@@ -990,11 +1009,16 @@ int export_upper_impl(risqgpu* h, int64_t* rowptr, int64_t* cols, double* vals, 
         for (size_t k = 0; k < h->cap; k++) v[k] = (double)hi[k] + (lo.empty() ? 0.0 : (double)lo[k]);
     }
     // count per caller row
+    // full rows hold each pair twice (keep the caller-order upper one); upper storage
+    // holds it once in internal order, which maps to (min, max) in caller order
     std::vector<int64_t> cnt(n + 1, 0);
     for (size_t p = 0; p < n; p++) {
         int64_t r = orig[p];
-        for (int64_t k = rs[p]; k < rs[p] + rl[p]; k++)
-            if (orig[ci[k]] > r) cnt[r]++;
+        for (int64_t k = rs[p]; k < rs[p] + rl[p]; k++) {
+            int64_t c = orig[ci[k]];
+            if (h->upper) cnt[std::min(r, c)]++;
+            else if (c > r) cnt[r]++;
+        }
     }
     rowptr[0] = 0;
     for (size_t r = 0; r < n; r++) rowptr[r + 1] = rowptr[r] + cnt[r];
@@ -1003,7 +1027,11 @@ int export_upper_impl(risqgpu* h, int64_t* rowptr, int64_t* cols, double* vals, 
         int64_t r = orig[p];
         for (int64_t k = rs[p]; k < rs[p] + rl[p]; k++) {
             int64_t c = orig[ci[k]];
-            if (c > r) { cols[fill[r]] = c; vals[fill[r]] = v[k]; fill[r]++; }
+            if (!h->upper && c <= r) continue;
+            const int64_t lo = std::min(r, c), hi = std::max(r, c);
+            cols[fill[lo]] = hi;
+            vals[fill[lo]] = v[k];
+            fill[lo]++;
         }
     }
     std::vector<std::pair<int64_t, double>> tmp;

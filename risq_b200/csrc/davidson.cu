@@ -475,6 +475,10 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         h->err = "the FP32 sigma of MIXED / FP32 mode needs an FP32 or MIXED build";
         return RISQGPU_ERR_INVALID;
     }
+    if (h->upper && h->precision == RISQGPU_FP32 && mode != RISQGPU_MODE_FP32) {
+        h->err = "an FP32 upper-triangle build has no FP64 sigma; use MIXED_UPPER or FP32 mode";
+        return RISQGPU_ERR_INVALID;
+    }
     if (precond == RISQGPU_PRECOND_LEARNED && !h->mlp.loaded) {
         h->err = "learned preconditioner requested but no MLP loaded";
         return RISQGPU_ERR_INVALID;

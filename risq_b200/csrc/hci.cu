@@ -250,7 +250,9 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
         // sparse_optimize (src/var/davidson.rs:43-113)
         const size_t N = h->wf_diag.size();
         if (!(h->built && added == 0)) {
-            RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, n_stored, h->wf_diag.data()));
+            // upper-triangle storage is rebuilt from scratch every time
+            const size_t nsh = cur_prec >= RISQGPU_FP64_UPPER ? 0 : n_stored;
+            RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, nsh, h->wf_diag.data()));
             int rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
             if (rc == RISQGPU_ERR_OOM && n_stored > 0) {
                 // no room for the kept previous matrix next to the new one: rebuild every pair
@@ -261,8 +263,15 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
                 rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
             }
             if (rc == RISQGPU_ERR_OOM && auto_prec && cur_prec == RISQGPU_FP64) {
-                // FP64 values do not fit: keep the columns only and recompute the FP64
-                // elements inside sigma (the same values, a quarter of the storage)
+                // both triangles do not fit: store each pair once (the reference's own layout)
+                if (verbose) std::fprintf(stderr, "[risqgpu] iter %d: full FP64 rows do not fit, upper triangle from here\n", iter);
+                cur_prec = RISQGPU_FP64_UPPER;
+                RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, 0, h->wf_diag.data()));
+                rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
+            }
+            if (rc == RISQGPU_ERR_OOM && auto_prec && cur_prec == RISQGPU_FP64_UPPER) {
+                // FP64 values do not fit at all: keep the columns only and recompute the FP64
+                // elements inside sigma (the same values, a third of the storage)
                 if (verbose) std::fprintf(stderr, "[risqgpu] iter %d: FP64 values do not fit, columns only from here\n", iter);
                 cur_prec = RISQGPU_COLS;
                 RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, 0, h->wf_diag.data()));

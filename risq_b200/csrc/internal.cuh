@@ -74,13 +74,15 @@ struct risqgpu {
     int32_t* d_gb = nullptr;        // group of each det (internal index)
     int32_t* d_gb_start = nullptr;  // G_b + 1 (positions in order_b)
     int32_t* d_order_b = nullptr;
+    int32_t* d_pos_b = nullptr;     // position of each det in order_b
     // single-excitation partners between alpha groups
     int32_t* d_pa_start = nullptr;  // G_a + 1
     int32_t* d_pa_list = nullptr;
     size_t n_pa = 0;
 
     // sparse H: both triangles, rows in internal order, diagonal separate
-    int precision = -1;
+    int precision = -1;   // value storage: FP64, FP32, MIXED or COLS
+    bool upper = false;   // only pairs with q > p (internal order) are stored
     bool built = false;
     int64_t* d_row_start = nullptr;  // N + 1 (segment starts; capacity per row)
     int32_t* d_row_len = nullptr;    // stored elements per row

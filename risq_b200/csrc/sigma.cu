@@ -143,6 +143,52 @@ int launch_otf(risqgpu* h, const double* x, double* y) {
     return check_launch(h, "sigma otf");
 }
 
+// Upper-triangle storage: y = diag * x first, then every stored pair (p, q > p)
+// adds v x_q to y_p (warp sum, one atomic per row) and v x_p to y_q (one atomic per
+// element; y stays in L2).  V: value type (double, float, or float + float
+// remainder when VLO); X: vector type.
+template <typename X>
+__global__ void k_diag_times(int64_t N, const double* __restrict__ diag, const X* __restrict__ x, X* __restrict__ y) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
+        y[p] = (X)(diag[p] * (double)x[p]);
+}
+
+template <typename V, typename X, bool VLO>
+__global__ void __launch_bounds__(256) k_spmv_upper(int64_t N, const int64_t* __restrict__ row_start,
+                                                    const int32_t* __restrict__ row_len,
+                                                    const int32_t* __restrict__ cols, const V* __restrict__ vals,
+                                                    const float* __restrict__ vlo, const X* __restrict__ x,
+                                                    X* __restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t p = warp; p < N; p += nwarps) {
+        const int64_t s = row_start[p];
+        const int len = row_len[p];
+        const X xp = x[p];
+        X acc = 0;
+        int k = lane;
+        for (; k + 32 < len; k += 64) {
+            const int c0 = __ldcs(cols + s + k), c1 = __ldcs(cols + s + k + 32);
+            X v0 = (X)__ldcs(vals + s + k), v1 = (X)__ldcs(vals + s + k + 32);
+            if constexpr (VLO) { v0 += (X)__ldcs(vlo + s + k); v1 += (X)__ldcs(vlo + s + k + 32); }
+            acc += v0 * __ldg(x + c0);
+            acc += v1 * __ldg(x + c1);
+            atomicAdd(y + c0, v0 * xp);
+            atomicAdd(y + c1, v1 * xp);
+        }
+        for (; k < len; k += 32) {
+            const int c = __ldcs(cols + s + k);
+            X v = (X)__ldcs(vals + s + k);
+            if constexpr (VLO) v += (X)__ldcs(vlo + s + k);
+            acc += v * __ldg(x + c);
+            atomicAdd(y + c, v * xp);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) atomicAdd(y + p, acc);
+    }
+}
+
 __global__ void k_permute_in(const double* __restrict__ x, const int32_t* __restrict__ orig, int64_t n,
                              double* __restrict__ xi) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
@@ -171,6 +217,25 @@ int sigma_device(risqgpu* h, const void* x, void* y, int kind) {
     if (!h->built) { h->err = "sigma before build"; return RISQGPU_ERR_INVALID; }
     const int64_t n = (int64_t)h->N;
     const int grid = spmv_grid(h);
+    if (h->upper) {
+        const int g1 = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
+        if (kind == 0) {
+            if (h->precision == RISQGPU_FP32) { h->err = "FP64 sigma needs FP64 or FP32 + remainder values"; return RISQGPU_ERR_INVALID; }
+            k_diag_times<double><<<g1, 256, 0, h->stream>>>(n, h->d_diag, (const double*)x, (double*)y);
+            if (h->precision == RISQGPU_FP64)
+                k_spmv_upper<double, double, false><<<grid, 256, 0, h->stream>>>(
+                    n, h->d_row_start, h->d_row_len, h->d_cols, h->d_val64, nullptr, (const double*)x, (double*)y);
+            else
+                k_spmv_upper<float, double, true><<<grid, 256, 0, h->stream>>>(
+                    n, h->d_row_start, h->d_row_len, h->d_cols, h->d_val32, h->d_val_lo, (const double*)x, (double*)y);
+        } else {
+            if (h->precision == RISQGPU_FP64) { h->err = "FP32 sigma needs FP32 values"; return RISQGPU_ERR_INVALID; }
+            k_diag_times<float><<<g1, 256, 0, h->stream>>>(n, h->d_diag, (const float*)x, (float*)y);
+            k_spmv_upper<float, float, false><<<grid, 256, 0, h->stream>>>(
+                n, h->d_row_start, h->d_row_len, h->d_cols, h->d_val32, nullptr, (const float*)x, (float*)y);
+        }
+        return check_launch(h, "sigma upper");
+    }
     if (kind == 0) {
         const double* xd = (const double*)x;
         double* yd = (double*)y;

@@ -246,3 +246,36 @@ def test_columns_only_build_and_recomputed_sigma(name):
         assert 0 < m.stats["n_sigma_fp64"] < m.stats["n_sigma"]
         f = g.davidson(1, None, 1e-4, 1e-8, 50, mode=_capi.MODE_FP32)
         assert f.converged and f.stats["n_sigma_fp64"] == 0
+
+
+@pytest.mark.parametrize("name", ["be2", "f2"])
+def test_upper_triangle_storage(name):
+    """FP64_UPPER / MIXED_UPPER store each pair once (SparseMatUpperTri's layout) and
+    add the transposed half with atomics: same set and values, same sigma to rounding."""
+    ints, p = H.golden_system(name)
+    _, dets, coeffs, diag, _ = H.oracle_hci(name)
+    x = np.random.default_rng(9).standard_normal(len(dets))
+    with _gpu(ints) as g:
+        g.set_dets(dets, 0, diag)
+        g.build(_capi.FP64)
+        ref_csr = g.export_upper()
+        ref_y = g.matrix_vector_prod(x)
+        r64 = g.davidson(1, None, 1e-4, 1e-8, 50)
+        st = g.build(_capi.FP64_UPPER)
+        assert st["nnz_upper"] == len(ref_csr[1])
+        for a, b in zip(g.export_upper(), ref_csr):
+            np.testing.assert_array_equal(a, b)
+        y = g.matrix_vector_prod(x)
+        assert np.max(np.abs(y - ref_y)) <= 1e-12 * np.max(np.abs(ref_y))
+        r = g.davidson(1, None, 1e-4, 1e-8, 50)
+        assert abs(r.eigenvalues[0] - r64.eigenvalues[0]) < 1e-9
+        g.build(_capi.MIXED_UPPER)
+        m = g.davidson(1, None, 1e-4, 1e-8, 50, mode=_capi.MODE_MIXED)
+        assert m.converged and abs(m.eigenvalues[0] - r64.eigenvalues[0]) < 1e-6
+        g.build(_capi.FP32_UPPER)
+        f = g.davidson(1, None, 1e-4, 1e-8, 50, mode=_capi.MODE_FP32)
+        assert f.converged and abs(f.eigenvalues[0] - r64.eigenvalues[0]) < 1e-4
+        with pytest.raises(_capi.RisqGpuError):
+            g.davidson(1, None, 1e-4, 1e-8, 50, mode=_capi.MODE_MIXED)  # FP32 upper has no FP64 sigma
+        with pytest.raises(_capi.RisqGpuError):
+            g.set_dets(dets, len(dets), diag)  # no incremental extension of an upper build
