@@ -242,10 +242,36 @@ RISQGPU_API int risqgpu_sigma_noalloc(risqgpu_t* h, const double* x_dev, double*
 RISQGPU_API int risqgpu_ham_diag(risqgpu_t* h, const uint64_t* dets, size_t n, double* out);
 RISQGPU_API int risqgpu_ham_off_diag(risqgpu_t* h, const uint64_t* d1, const uint64_t* d2, size_t n, double* out);
 
-/* Learned preconditioner: load MLP weights ((2n+2) -> 128 -> 128 -> 1, FP32
- * master copy; the device runs BF16 weights with FP32 accumulation). */
+/* Learned preconditioner (no counterpart in the reference, which has DPR only):
+ * an MLP (2n+2) -> hidden -> hidden -> 1 (ReLU) gives each determinant a factor
+ * f = clamp(exp(out), 0.25, 4) applied to its DPR step r_i / (lambda - H_ii).
+ * Features: 2n occupations as +1/-1 (alpha orbitals, then beta), then
+ * (H_ii - E - mu_e) * s_e and (sum of occupied h_pp - mu_h) * s_h with
+ * feat_norm = {mu_e, s_e, mu_h, s_h} (NULL = {0, 1, 0, 1}).  Weights are row-major
+ * FP32 (W1: hidden x n_in, W2: hidden x hidden, W3: 1 x hidden); the device rounds
+ * them to BF16 and accumulates in FP32. */
 RISQGPU_API int risqgpu_set_precond_mlp(risqgpu_t* h, int n_in, int hidden, const float* w1, const float* b1,
-                            const float* w2, const float* b2, const float* w3, const float* b3);
+                            const float* w2, const float* b2, const float* w3, const float* b3,
+                            const float* feat_norm);
+
+/* Per-determinant preconditioner factors of the loaded MLP for energy E, caller
+ * order (N floats).  For checking the network against a CPU evaluation. */
+RISQGPU_API int risqgpu_precond_factors(risqgpu_t* h, double energy, float* out);
+
+/* MLP training on the device (forward and backward kernels of this library, Adam).
+ * params: packed FP32 [W1 (H x n_in), b1 (H), W2 (H x H), b2 (H), W3 (H), b3 (1)];
+ * feats: B x n_in features (already normalised), target: B factors, weight: B
+ * sample weights.  Loss L = sum_b w_b (exp(o_b) - t_b)^2 / sum_b w_b, with o the
+ * network output computed from BF16-rounded weights.
+ * risqgpu_mlp_grad: L and dL/dparams (FP32, straight through the rounding) for
+ * one batch.  risqgpu_mlp_train: `epochs` passes of Adam (lr, betas 0.9/0.999)
+ * over shuffled minibatches of `batch` rows; params updated in place; loss_hist
+ * (epochs entries, nullable) receives the mean loss of each epoch. */
+RISQGPU_API int risqgpu_mlp_grad(int device, int n_in, int hidden, const float* params, const float* feats,
+                                 const float* target, const float* weight, int64_t B, float* loss, float* grad);
+RISQGPU_API int risqgpu_mlp_train(int device, int n_in, int hidden, float* params, const float* feats,
+                                  const float* target, const float* weight, int64_t B, int epochs, int batch,
+                                  float lr, uint64_t seed, float* loss_hist);
 
 #ifdef __cplusplus
 }

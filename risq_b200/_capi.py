@@ -90,7 +90,11 @@ SIGNATURES = [
     ("risqgpu_sigma_noalloc", C.c_int, [_handle, C.c_void_p, C.c_void_p]),
     ("risqgpu_ham_diag", C.c_int, [_handle, _u64p, C.c_size_t, _dp]),
     ("risqgpu_ham_off_diag", C.c_int, [_handle, _u64p, _u64p, C.c_size_t, _dp]),
-    ("risqgpu_set_precond_mlp", C.c_int, [_handle, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _fp, _fp]),
+    ("risqgpu_set_precond_mlp", C.c_int, [_handle, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _fp, _fp, _fp]),
+    ("risqgpu_precond_factors", C.c_int, [_handle, C.c_double, _fp]),
+    ("risqgpu_mlp_grad", C.c_int, [C.c_int, C.c_int, C.c_int, _fp, _fp, _fp, _fp, C.c_int64, _fp, _fp]),
+    ("risqgpu_mlp_train", C.c_int, [C.c_int, C.c_int, C.c_int, _fp, _fp, _fp, _fp, C.c_int64, C.c_int, C.c_int,
+                                    C.c_float, C.c_uint64, _fp]),
     ("risqgpu_find_new_dets", C.c_int, [_handle, _dp, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_size_t)]),
     ("risqgpu_get_new_dets", C.c_int, [_handle, _u64p, _dp, C.c_size_t]),
     ("risqgpu_variational", C.c_int, [_handle, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,

@@ -190,10 +190,16 @@ int risqgpu_ham_off_diag(risqgpu_t* h, const uint64_t* d1, const uint64_t* d2, s
 }
 
 int risqgpu_set_precond_mlp(risqgpu_t* h, int n_in, int hidden, const float* w1, const float* b1, const float* w2,
-                            const float* b2, const float* w3, const float* b3) {
+                            const float* b2, const float* w3, const float* b3, const float* feat_norm) {
     if (!h) return RISQGPU_ERR_INVALID;
     DeviceGuard g(h->device);
-    return set_mlp_impl(h, n_in, hidden, w1, b1, w2, b2, w3, b3);
+    return set_mlp_impl(h, n_in, hidden, w1, b1, w2, b2, w3, b3, feat_norm);
+}
+
+int risqgpu_precond_factors(risqgpu_t* h, double energy, float* out) {
+    if (!h || !out) return RISQGPU_ERR_INVALID;
+    DeviceGuard g(h->device);
+    return precond_factors_impl(h, energy, out);
 }
 
 }  // extern "C"

@@ -388,7 +388,7 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
                                    h->stream));
         // learned scaling: refresh the per-determinant factors when the energy used in
         // their features moved by more than 10 mHa; fall back to plain DPR for an
-        // iteration whenever the residual did not drop by 10% over the last one
+        // iteration whenever the residual stalled (no new minimum in the last 3 iterations)
         const float* fs = nullptr;
         if (fscale) {
             if (std::isnan(e_feat) || std::fabs(w[0] - e_feat) > 1e-2) {
@@ -396,7 +396,13 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
                 RQ_TRY(mlp_scale_impl(h, e_feat, fscale));
             }
             const size_t k = res_hist.size();
-            bool stalled = k >= 2 && !(res_hist[k - 1] < 0.9 * res_hist[k - 2]);
+            bool stalled = false;
+            if (k >= 4) {
+                double best_before = res_hist[0];
+                for (size_t j = 1; j + 3 < k; j++) best_before = std::min(best_before, res_hist[j]);
+                double best_recent = std::min(res_hist[k - 1], std::min(res_hist[k - 2], res_hist[k - 3]));
+                stalled = !(best_recent < best_before);
+            }
             if (stalled) out.fallbacks++;
             else fs = fscale;
         }

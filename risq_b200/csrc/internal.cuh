@@ -32,6 +32,7 @@ struct MlpWeights {
     // device copies: bf16 weights as raw u16 + fp32 biases
     uint16_t *w1 = nullptr, *w2 = nullptr, *w3 = nullptr;
     float *b1 = nullptr, *b2 = nullptr, *b3 = nullptr;
+    float4 fnorm = {0.f, 1.f, 0.f, 1.f};  // (mu_e, 1/sd_e, mu_h, 1/sd_h)
     bool loaded = false;
 };
 
@@ -184,7 +185,8 @@ int sigma_host(risqgpu* h, const double* x, double* y, int nvec);
 int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double tol, double etol, int max_iter,
                   int mode, int precond, double* evals, double* evecs, risqgpu_dstats* st);
 int set_mlp_impl(risqgpu* h, int n_in, int hidden, const float* w1, const float* b1, const float* w2,
-                 const float* b2, const float* w3, const float* b3);
+                 const float* b2, const float* w3, const float* b3, const float* feat_norm);
 void free_mlp(risqgpu* h);
+int precond_factors_impl(risqgpu* h, double energy, float* out);
 
 }  // namespace risq

@@ -3,9 +3,11 @@
 // The network maps determinant features to a multiplicative correction of the
 // DPR step r_i / (lambda - H_ii): f_i = clamp(exp(MLP(x_i)), 0.25, 4).
 // Features x_i (2n + 2 values, n = orbitals): occupation of each alpha orbital
-// then each beta orbital as +1 / -1, H_ii - E, and the sum of h_pp over the
-// occupied spin-orbitals.  Layers (2n+2) -> hidden -> hidden -> 1 with ReLU;
-// weights are held in BF16 on the device and every product accumulates in FP32.
+// then each beta orbital as +1 / -1, (H_ii - E - mu_e) * s_e, and
+// (sum of h_pp over the occupied spin-orbitals - mu_h) * s_h, where (mu_e, s_e,
+// mu_h, s_h) are the network's feature normalisation.  Layers
+// (2n+2) -> hidden -> hidden -> 1 with ReLU; weights are rounded to BF16 (round
+// to nearest even) on the device and every product accumulates in FP32.
 // There is no counterpart in the reference (which only has DPR,
 // algorithms/davidson.rs:391-408); the reference's DPR is the fallback.
 #include <algorithm>
@@ -42,7 +44,7 @@ __global__ void __launch_bounds__(128) k_mlp_scale(const uint64_t* __restrict__ 
                                                    const uint16_t* __restrict__ w1, const float* __restrict__ b1,
                                                    const uint16_t* __restrict__ w2, const float* __restrict__ b2,
                                                    const uint16_t* __restrict__ w3, const float* __restrict__ b3,
-                                                   float* __restrict__ out) {
+                                                   float4 fnorm, float* __restrict__ out) {
     extern __shared__ float sm[];
     float* W1 = sm;                      // hidden x n_in
     float* W2 = W1 + hidden * n_in;      // hidden x hidden
@@ -71,7 +73,8 @@ __global__ void __launch_bounds__(128) k_mlp_scale(const uint64_t* __restrict__ 
             if ((a[o >> 6] >> (o & 63)) & 1ull) sum_h += HPP[o];
             if ((b[o >> 6] >> (o & 63)) & 1ull) sum_h += HPP[o];
         }
-        const float dE = (float)(diag[p] - energy);
+        const float dE = ((float)(diag[p] - energy) - fnorm.x) * fnorm.y;
+        sum_h = (sum_h - fnorm.z) * fnorm.w;
         float hid[HMAX];
 #pragma unroll
         for (int j = 0; j < HMAX; j++) {
@@ -110,7 +113,7 @@ void free_mlp(risqgpu* h) {
 }
 
 int set_mlp_impl(risqgpu* h, int n_in, int hidden, const float* w1, const float* b1, const float* w2, const float* b2,
-                 const float* w3, const float* b3) {
+                 const float* w3, const float* b3, const float* feat_norm) {
     if (n_in != 2 * h->norb + 2) { h->err = "MLP input size must be 2*norb + 2"; return RISQGPU_ERR_INVALID; }
     if (hidden < 1 || hidden > HMAX) { h->err = "MLP hidden size must be in [1, 128]"; return RISQGPU_ERR_INVALID; }
     if (!w1 || !b1 || !w2 || !b2 || !w3 || !b3) { h->err = "null MLP weights"; return RISQGPU_ERR_INVALID; }
@@ -135,6 +138,8 @@ int set_mlp_impl(risqgpu* h, int n_in, int hidden, const float* w1, const float*
     RQ_TRY(up32(b3, 1, h->mlp.b3));
     h->mlp.n_in = n_in;
     h->mlp.hidden = hidden;
+    h->mlp.fnorm = feat_norm ? make_float4(feat_norm[0], feat_norm[1], feat_norm[2], feat_norm[3])
+                             : make_float4(0.f, 1.f, 0.f, 1.f);
     h->mlp.loaded = true;
     return RISQGPU_OK;
 }
@@ -149,14 +154,36 @@ int mlp_scale_impl(risqgpu* h, double energy, float* out) {
         RQ_CUDA(h, cudaFuncSetAttribute(k_mlp_scale<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_mlp_scale<1><<<grid, 128, smem, h->stream>>>(h->d_up, h->d_dn, h->d_diag, N, h->norb, h->d_h1, energy, nin,
                                                        hid, h->mlp.w1, h->mlp.b1, h->mlp.w2, h->mlp.b2, h->mlp.w3,
-                                                       h->mlp.b3, out);
+                                                       h->mlp.b3, h->mlp.fnorm, out);
     } else {
         RQ_CUDA(h, cudaFuncSetAttribute(k_mlp_scale<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_mlp_scale<2><<<grid, 128, smem, h->stream>>>(h->d_up, h->d_dn, h->d_diag, N, h->norb, h->d_h1, energy, nin,
                                                        hid, h->mlp.w1, h->mlp.b1, h->mlp.w2, h->mlp.b2, h->mlp.w3,
-                                                       h->mlp.b3, out);
+                                                       h->mlp.b3, h->mlp.fnorm, out);
     }
     return check_launch(h, "mlp scale");
+}
+
+__global__ void k_factors_to_caller(const float* __restrict__ fi, const int32_t* __restrict__ orig, int64_t n,
+                                    float* __restrict__ fc) {
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+        fc[orig[p]] = fi[p];
+}
+
+int precond_factors_impl(risqgpu* h, double energy, float* out) {
+    if (h->N == 0) { h->err = "no determinants set"; return RISQGPU_ERR_INVALID; }
+    const int64_t n = (int64_t)h->N;
+    float *fi = nullptr, *fc = nullptr;
+    RQ_TRY(dalloc(h, fi, n));
+    RQ_TRY(dalloc(h, fc, n));
+    RQ_TRY(mlp_scale_impl(h, energy, fi));
+    k_factors_to_caller<<<(int)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, h->stream>>>(fi, h->d_orig, n, fc);
+    RQ_TRY(check_launch(h, "factors"));
+    RQ_CUDA(h, cudaMemcpyAsync(out, fc, sizeof(float) * n, cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "factors"));
+    dfree(fi);
+    dfree(fc);
+    return RISQGPU_OK;
 }
 
 }  // namespace risq

@@ -160,8 +160,10 @@ class GpuHam:
             A.check(rc, self._h)
         return DavidsonResult(ev, vecs.T.copy(), st.as_dict(), rc == A.OK)
 
-    def set_precond_mlp(self, w1, b1, w2, b2, w3, b3):
-        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (w1, b1, w2, b2, w3, b3)]
+    def set_precond_mlp(self, w1, b1, w2, b2, w3, b3, feat_norm=(0.0, 1.0, 0.0, 1.0)):
+        """Load the learned-preconditioner network (risqgpu_set_precond_mlp).  feat_norm =
+        (shift, scale) for the H_ii - E feature, then for the occupied-h_pp feature."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float32) for a in (w1, b1, w2, b2, w3, b3, feat_norm)]
         hidden, n_in = arrs[0].shape
         A.check(A.lib().risqgpu_set_precond_mlp(self._h, n_in, hidden, *[A.ptr(a, A._fp) for a in arrs]), self._h)
 

@@ -1,0 +1,272 @@
+"""Learned correction of the Davidson diagonal preconditioner.
+
+The reference's Davidson uses DPR, t = r / (lambda - H_ii)
+(src/var/eigenvalues/algorithms/davidson.rs:391-408).  Here a small network gives
+each determinant a factor f in [0.25, 4] and the step becomes f * r / (lambda - H_ii);
+DPR stays the fallback whenever the residual stalls (risq_b200/csrc/davidson.cu).
+
+Training data are residual -> exact-correction pairs from FP64 Davidson runs:
+along a DPR trajectory (x_k, lambda_k, r_k) of a training system whose converged
+eigenvector x* is known, the ideal update is e = x* / (x*.x_k) - x_k; the DPR step is
+t = r_k / (lambda_k - H_ii); the target factor of determinant i is
+e_i / (a t_i), a = (e.t) / (t.t), clipped to [0.25, 4], and the sample weight is
+(a t_i)^2, so that the weighted loss is the squared error of the corrected step.
+Training runs on the device with this library's forward / backward kernels.
+
+Features (the inference kernel computes the same, mlp.cu): 2n occupations as +1/-1
+(alpha orbitals, then beta), (H_ii - E - mu_e) * s_e and
+(sum of occupied h_pp - mu_h) * s_h.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+
+import numpy as np
+
+from . import _capi as A
+from .fcidump import Integrals, dets_to_ints
+
+HIDDEN = 128
+DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+
+
+@dataclasses.dataclass
+class PrecondMLP:
+    norb: int
+    hidden: int
+    params: np.ndarray   # packed float32 [W1, b1, W2, b2, W3, b3]
+    fnorm: np.ndarray    # float32 [mu_e, s_e, mu_h, s_h]
+
+    @property
+    def n_in(self):
+        return 2 * self.norb + 2
+
+    @classmethod
+    def init(cls, norb, hidden=HIDDEN, seed=0, fnorm=None):
+        n_in = 2 * norb + 2
+        rng = np.random.default_rng(seed)
+        W1 = rng.standard_normal((hidden, n_in)) * np.sqrt(2.0 / n_in)
+        W2 = rng.standard_normal((hidden, hidden)) * np.sqrt(2.0 / hidden)
+        W3 = rng.standard_normal(hidden) * np.sqrt(1.0 / hidden) * 0.1
+        p = np.concatenate([W1.ravel(), np.zeros(hidden), W2.ravel(), np.zeros(hidden), W3, [0.0]]).astype(np.float32)
+        fn = np.asarray(fnorm if fnorm is not None else [0.0, 1.0, 0.0, 1.0], dtype=np.float32)
+        return cls(norb, hidden, p, fn)
+
+    def split(self):
+        H, n = self.hidden, self.n_in
+        p = self.params
+        o = 0
+        W1 = p[o:o + H * n].reshape(H, n); o += H * n
+        b1 = p[o:o + H]; o += H
+        W2 = p[o:o + H * H].reshape(H, H); o += H * H
+        b2 = p[o:o + H]; o += H
+        W3 = p[o:o + H]; o += H
+        b3 = p[o:o + 1]
+        return W1, b1, W2, b2, W3, b3
+
+    def save(self, path):
+        np.savez(path, norb=self.norb, hidden=self.hidden, params=self.params, fnorm=self.fnorm)
+
+    @classmethod
+    def load(cls, path):
+        z = np.load(path)
+        return cls(int(z["norb"]), int(z["hidden"]), z["params"].astype(np.float32), z["fnorm"].astype(np.float32))
+
+
+def default_model_path(norb):
+    return os.path.join(DATA_DIR, f"precond_mlp_n{norb}.npz")
+
+
+def load_default(norb):
+    path = default_model_path(norb)
+    return PrecondMLP.load(path) if os.path.exists(path) else None
+
+
+def install(gpu, model: PrecondMLP):
+    """Load the network into a GpuHam handle (risqgpu_set_precond_mlp)."""
+    W1, b1, W2, b2, W3, b3 = (np.ascontiguousarray(a, dtype=np.float32) for a in model.split())
+    fn = np.ascontiguousarray(model.fnorm, dtype=np.float32)
+    A.check(A.lib().risqgpu_set_precond_mlp(gpu._h, model.n_in, model.hidden, A.ptr(W1, A._fp), A.ptr(b1, A._fp),
+                                            A.ptr(W2, A._fp), A.ptr(b2, A._fp), A.ptr(W3, A._fp), A.ptr(b3, A._fp),
+                                            A.ptr(fn, A._fp)), gpu._h)
+
+
+def device_factors(gpu, energy):
+    out = np.zeros(gpu.n, dtype=np.float32)
+    A.check(A.lib().risqgpu_precond_factors(gpu._h, energy, A.ptr(out, A._fp)), gpu._h)
+    return out
+
+
+def raw_features(dets, diag, energy, ints: Integrals):
+    """(N, 2n+2) float32 features before normalisation of the last two columns."""
+    n = ints.norb
+    d = np.asarray(dets, dtype=np.uint64)
+    N = d.shape[0]
+    hpp = np.array([ints.h(k, k) for k in range(n)], dtype=np.float32)
+    out = np.empty((N, 2 * n + 2), dtype=np.float32)
+    up = np.zeros((N, n), dtype=bool)
+    dn = np.zeros((N, n), dtype=bool)
+    for k in range(n):
+        word, bit = k // 64, np.uint64(k % 64)
+        up[:, k] = ((d[:, word] >> bit) & np.uint64(1)).astype(bool)
+        dn[:, k] = ((d[:, 2 + word] >> bit) & np.uint64(1)).astype(bool)
+    out[:, :n] = np.where(up, 1.0, -1.0)
+    out[:, n:2 * n] = np.where(dn, 1.0, -1.0)
+    out[:, 2 * n] = (np.asarray(diag, dtype=np.float64) - energy).astype(np.float32)
+    out[:, 2 * n + 1] = (up.astype(np.float32) @ hpp) + (dn.astype(np.float32) @ hpp)
+    return out
+
+
+def normalise(feats, fnorm):
+    f = feats.copy()
+    n2 = f.shape[1] - 2
+    f[:, n2] = (f[:, n2] - fnorm[0]) * fnorm[1]
+    f[:, n2 + 1] = (f[:, n2 + 1] - fnorm[2]) * fnorm[3]
+    return f
+
+
+def dpr_trajectory(sigma, diag, tol=1e-4, etol=1e-8, max_iter=1000, record=None):
+    """DPR Davidson (the reference's algorithm, one root, default start with identity
+    columns 0 and 1) in FP64 numpy with a device sigma; record(k, lam, x, r) is called
+    at every iteration with the normalised Ritz vector and residual."""
+    N = len(diag)
+    mss = min(11, N)
+    V = np.zeros((N, mss))
+    V[0, 0] = 1.0
+    V[1, 1] = 1.0
+    dim = 2
+    HV = np.zeros((N, mss))
+    for c in range(dim):
+        HV[:, c] = sigma(V[:, c])
+    last = 0.0
+    for it in range(max_iter):
+        P = V[:, :dim].T @ HV[:, :dim]
+        P = (P + P.T) / 2
+        w, Y = np.linalg.eigh(P)
+        lam, y = w[0], Y[:, 0]
+        x = V[:, :dim] @ y
+        hx = HV[:, :dim] @ y
+        r = hx - lam * x
+        if record is not None:
+            record(it, lam, x, r)
+        if np.linalg.norm(r) < tol and abs(lam - last) < etol:
+            return lam, x, it + 1
+        last = lam
+        if dim + 1 <= mss:
+            t = r / (lam - diag)
+            for _ in range(2):
+                t -= V[:, :dim] @ (V[:, :dim].T @ t)
+            t /= np.linalg.norm(t)
+            V[:, dim] = t
+            HV[:, dim] = sigma(t)
+            dim += 1
+        else:
+            V[:, 0] = x / np.linalg.norm(x)
+            HV[:, 0] = hx / np.linalg.norm(x)
+            dim = 1
+    return lam, x, max_iter
+
+
+def correction_samples(gpu, dets, diag, ints, per_iter=2000, rng=None, max_iter=1000):
+    """Residual -> exact-correction samples of one training system (FP64 Davidson)."""
+    rng = rng or np.random.default_rng(0)
+    sigma = gpu.matrix_vector_prod
+    # converged reference eigenvector
+    lam_star, x_star, _ = dpr_trajectory(sigma, diag, tol=1e-7, etol=1e-12, max_iter=max_iter)
+    x_star = x_star / np.linalg.norm(x_star)
+    feats, targets, weights = [], [], []
+
+    def record(k, lam, x, r):
+        nx = np.linalg.norm(x)
+        x = x / nx
+        r = r / nx
+        ov = x_star @ x
+        if abs(ov) < 0.3:
+            return
+        e = x_star / ov - x
+        t = r / (lam - diag)
+        tt = t @ t
+        if tt <= 0:
+            return
+        a = (e @ t) / tt
+        if a == 0:
+            return
+        at = a * t
+        with np.errstate(divide="ignore", invalid="ignore"):
+            f = np.where(np.abs(at) > 0, e / at, 1.0)
+        f = np.clip(np.nan_to_num(f, nan=1.0, posinf=4.0, neginf=0.25), 0.25, 4.0)
+        w = at * at
+        s = w.sum()
+        if not s > 0:
+            return
+        m = min(per_iter, len(diag))
+        idx = rng.choice(len(diag), size=m, replace=False, p=w / s)
+        raw = raw_features(dets[idx], diag[idx], lam, ints)
+        feats.append(raw)
+        targets.append(f[idx].astype(np.float32))
+        weights.append(np.ones(m, dtype=np.float32))
+
+    dpr_trajectory(sigma, diag, tol=1e-4, etol=1e-8, max_iter=max_iter, record=record)
+    if not feats:
+        return None
+    return np.concatenate(feats), np.concatenate(targets), np.concatenate(weights)
+
+
+def grad(model: PrecondMLP, feats, target, weight, device=0):
+    """Loss and gradient of one batch on the device (risqgpu_mlp_grad)."""
+    X = np.ascontiguousarray(feats, dtype=np.float32)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    w = np.ascontiguousarray(weight, dtype=np.float32)
+    p = np.ascontiguousarray(model.params, dtype=np.float32)
+    g = np.zeros_like(p)
+    loss = C.c_float()
+    A.check(A.lib().risqgpu_mlp_grad(device, model.n_in, model.hidden, A.ptr(p, A._fp), A.ptr(X, A._fp),
+                                     A.ptr(t, A._fp), A.ptr(w, A._fp), X.shape[0], C.byref(loss), A.ptr(g, A._fp)))
+    return loss.value, g
+
+
+def train(model: PrecondMLP, feats, target, weight, epochs=20, batch=4096, lr=1e-3, seed=0, device=0):
+    """Adam on the device (risqgpu_mlp_train); returns the per-epoch loss."""
+    X = np.ascontiguousarray(feats, dtype=np.float32)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    w = np.ascontiguousarray(weight, dtype=np.float32)
+    p = np.ascontiguousarray(model.params, dtype=np.float32).copy()
+    hist = np.zeros(epochs, dtype=np.float32)
+    A.check(A.lib().risqgpu_mlp_train(device, model.n_in, model.hidden, A.ptr(p, A._fp), A.ptr(X, A._fp),
+                                      A.ptr(t, A._fp), A.ptr(w, A._fp), X.shape[0], epochs, batch, lr, seed,
+                                      A.ptr(hist, A._fp)))
+    model.params = p
+    return hist
+
+
+def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, device=0, per_iter=2000, log=print):
+    """systems: list of (ints, dets, diag).  Builds the samples, fits the feature
+    normalisation and trains a fresh network."""
+    from .gpu import GpuHam
+    F, T, Wt = [], [], []
+    rng = np.random.default_rng(seed)
+    for k, (ints, dets, diag) in enumerate(systems):
+        with GpuHam(ints, device) as g:
+            g.set_dets(dets, 0, diag)
+            g.build(A.FP64)
+            smp = correction_samples(g, dets, diag, ints, per_iter=per_iter, rng=rng)
+        if smp is None:
+            continue
+        F.append(smp[0]); T.append(smp[1]); Wt.append(smp[2])
+        log(f"# training system {k}: {len(dets)} dets, {len(smp[1])} samples")
+    raw = np.concatenate(F)
+    n2 = raw.shape[1] - 2
+    mu_e, sd_e = float(raw[:, n2].mean()), float(raw[:, n2].std() + 1e-6)
+    mu_h, sd_h = float(raw[:, n2 + 1].mean()), float(raw[:, n2 + 1].std() + 1e-6)
+    model = PrecondMLP.init(norb, seed=seed, fnorm=[mu_e, 1.0 / sd_e, mu_h, 1.0 / sd_h])
+    feats = normalise(raw, model.fnorm)
+    hist = train(model, feats, np.concatenate(T), np.concatenate(Wt), epochs=epochs, batch=batch, lr=lr, seed=seed,
+                 device=device)
+    return model, hist
+
+
+__all__ = ["PrecondMLP", "install", "device_factors", "raw_features", "normalise", "dpr_trajectory",
+           "correction_samples", "grad", "train", "train_from_systems", "load_default", "default_model_path",
+           "dets_to_ints"]

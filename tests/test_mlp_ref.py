@@ -1,0 +1,50 @@
+"""The CPU reference of the preconditioner MLP against finite differences (no GPU)."""
+import numpy as np
+
+from oracle import mlp_ref
+from risq_b200.learned import PrecondMLP, normalise, raw_features
+from risq_b200.fcidump import dets_from_ints, synthetic_integrals
+
+
+def test_bf16_round_ties_to_even():
+    x = np.array([1.0, 1.0 + 2**-8, 1.0 + 3 * 2**-8, -2.5, 3.1415927], dtype=np.float32)
+    r = mlp_ref.bf16_round(x)
+    assert r[0] == 1.0 and r[1] == 1.0          # exactly half an ulp: to even
+    assert r[2] == np.float32(1.0 + 4 * 2**-8)  # above half: up
+    assert r[3] == -2.5
+    assert abs(r[4] - 3.140625) < 1e-7
+
+
+def test_reference_gradient_by_finite_differences():
+    n_in, H = 6, 8
+    rng = np.random.default_rng(0)
+    m = PrecondMLP.init(2, hidden=H, seed=1)
+    # exercise the gradient away from BF16 rounding effects: use weights exact in BF16
+    p = mlp_ref.bf16_round(m.params)
+    X = rng.standard_normal((20, n_in))
+    t = rng.uniform(0.5, 2.0, 20)
+    w = rng.uniform(0.1, 1.0, 20)
+    loss, g = mlp_ref.loss_and_grad(p, X, t, w, n_in, H)
+    # biases are not rounded: finite differences on them are exact in the model
+    o = H * n_in
+    for k in list(range(o, o + H)) + [len(p) - 1]:
+        eps = 1e-3
+        pp = p.astype(np.float64).copy(); pp[k] += eps
+        pm = p.astype(np.float64).copy(); pm[k] -= eps
+        lp = mlp_ref.loss_and_grad(pp.astype(np.float32), X, t, w, n_in, H)[0]
+        lm = mlp_ref.loss_and_grad(pm.astype(np.float32), X, t, w, n_in, H)[0]
+        assert abs((lp - lm) / (2 * eps) - g[k]) < 1e-3 * max(1.0, abs(g[k]))
+
+
+def test_features_layout():
+    ints = synthetic_integrals(6, 0)
+    dets = dets_from_ints([(0b000111, 0b001011)])
+    f = raw_features(dets, np.array([-3.0]), -4.0, ints)
+    assert f.shape == (1, 14)
+    np.testing.assert_array_equal(f[0, :6], [1, 1, 1, -1, -1, -1])
+    np.testing.assert_array_equal(f[0, 6:12], [1, 1, -1, 1, -1, -1])
+    assert f[0, 12] == 1.0
+    hpp = [ints.h(k, k) for k in range(6)]
+    assert abs(f[0, 13] - (hpp[0] + hpp[1] + hpp[2] + hpp[0] + hpp[1] + hpp[3])) < 1e-5
+    g = normalise(f, np.array([1.0, 2.0, 0.0, 0.5], dtype=np.float32))
+    assert g[0, 12] == 0.0 and abs(g[0, 13] - 0.5 * f[0, 13]) < 1e-6
