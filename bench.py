@@ -4,15 +4,20 @@
 Workload (default --config 1): seeded synthetic integrals n = 20 orbitals,
 8 alpha + 8 beta electrons, seed 0, HCI threshold eps_var = 5e-5.  The
 determinant set is produced, outside the timed region, by this library's own
-variational stage on the device (cached under data/).  One timed step is one
-time-to-E_var solve over that set: FP64 sparse-H build followed by plain FP64
-Davidson (DPR preconditioner, the reference's algorithm) from the reference's
-default start until |r| < 1e-4 and |dE| < 1e-8.
+variational stage on the device (cached under data/).
+
+One timed step is one time-to-E_var solve over that set on the product path:
+sparse-H build with FP32 values + FP32 remainder, then Davidson with FP32 sigma
+and FP32 basis (FP64 dots, Gram-Schmidt and Rayleigh-Ritz), the learned
+preconditioner (DPR fallback), and closing FP64-sigma sweeps, from the
+reference's default start until |r| < 1e-4 and |dE| < 1e-8.  The plain FP64
+path (FP64 build + the reference's DPR Davidson) is timed beside it on the same
+set, and the energy difference of the two is reported (it must stay <= 1 uHa).
 
 Metric: determinants solved per second = N_dets * steps / time (max over ranks),
 whole job.  With N GPUs every rank solves its own replica (the single-GPU path
-does not shard), so scaling is weak.  Extra keys report sigma GB/s against the
-measured HBM peak, H-build elements/s, the mixed-precision solve and its |dE|.
+does not shard), so scaling is weak.  Extra keys: both solve times and their
+ratio, sigma GB/s against the measured HBM peak, H-build elements/s.
 """
 from __future__ import annotations
 
@@ -226,9 +231,13 @@ def main():
     g = GpuHam(ints, local)
     g.set_stream(stream.cuda_stream)
     ev = lambda: torch.cuda.Event(enable_timing=True)
-
-    # ---- device-resident time-to-E_var (FP64 build + plain DPR Davidson) ----
+    from risq_b200 import learned
+    model = learned.load_default(ints.norb)
+    if model is not None:
+        learned.install(g, model)
+    precond = _capi.PRECOND_LEARNED if model is not None else _capi.PRECOND_DPR
     g.set_dets(dets, 0, diag)
+
     def first_fitting(precs):
         for pr in precs:
             try:
@@ -240,26 +249,25 @@ def main():
                 say(f"# storage {pr} does not fit one GPU")
         raise RuntimeError("no storage mode fits")
 
-    # FP64 rows when both triangles fit; else the upper triangle (the reference's
-    # SparseMatUpperTri layout); else columns only with the elements recomputed in sigma
-    prec64 = first_fitting([_capi.FP64, _capi.FP64_UPPER, _capi.COLS])
-    energies, builds, davs = [], [], []
+    # product path storage: FP32 + FP32 remainder rows when both triangles fit, else the
+    # upper triangle (the reference's SparseMatUpperTri layout)
+    precm = first_fitting([_capi.MIXED, _capi.MIXED_UPPER])
+
+    def product_step():
+        hs = g.build(precm)
+        r = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=_capi.MODE_MIXED, precond=precond)
+        return hs, r
+
     clocks = ClockSampler(local)
     clocks.start()
     for i in range(args.warmup):
-        g.build(prec64)
-        g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
+        product_step()
     torch.cuda.synchronize()
     barrier()
     clocks.mark()
     t_start, t_end = ev(), ev()
     t_start.record(stream)
-    for i in range(args.steps):
-        hs = g.build(prec64)
-        r = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
-        energies.append(float(r.eigenvalues[0]))
-        builds.append(hs)
-        davs.append(r.stats)
+    runs = [product_step() for _ in range(args.steps)]
     t_end.record(stream)
     torch.cuda.synchronize()
     ms = t_start.elapsed_time(t_end) / args.steps
@@ -269,9 +277,88 @@ def main():
         dist.all_reduce(mx, op=dist.ReduceOp.MAX)
     ms_max = float(mx.item())
     barrier()
-    e64 = energies[-1]
-    dstat = davs[-1]
-    hstat = builds[-1]
+    hs_m, r_m = runs[-1]
+    e_m = float(r_m.eigenvalues[0])
+
+    # kernel launches of one product step, counted by CUPTI (torch.profiler) on an untimed step
+    launches_per_step = None
+    try:
+        from torch.profiler import ProfilerActivity, profile
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            product_step()
+            torch.cuda.synchronize()
+        launches_per_step = sum(1 for e in prof.events()
+                                if e.device_type.name == "CUDA" and e.name.startswith(("k_", "void risq::")))
+    except Exception as e:  # profiler unavailable: leave the count out rather than guess
+        say(f"# launch count unavailable: {e}")
+
+    # ---- mixed precision with the plain DPR preconditioner (one untimed-loop run) ----
+    a, b = ev(), ev()
+    torch.cuda.synchronize()
+    a.record(stream)
+    g.build(precm)
+    r_md = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=_capi.MODE_MIXED)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms_mixed_dpr = a.elapsed_time(b)
+
+    # ---- plain FP64 GPU path on the same set: FP64 build + the reference's DPR Davidson ----
+    prec64 = first_fitting([_capi.FP64, _capi.FP64_UPPER, _capi.COLS])
+    plain_ms, plain = [], None
+    for i in range(1 + max(1, min(args.steps, 2))):
+        a, b = ev(), ev()
+        torch.cuda.synchronize()
+        a.record(stream)
+        hs64 = g.build(prec64)
+        r64 = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i > 0:  # the first is a warm-up
+            plain_ms.append(a.elapsed_time(b))
+        plain = (hs64, r64)
+    hs64, r64 = plain
+    e64 = float(r64.eigenvalues[0])
+    ms_plain = float(np.mean(plain_ms))
+
+    # ---- sigma roofline, FP64 (x, y in the library's internal order) ----
+    nnz_u, nnz_f = g.nnz()
+    x = torch.randn(N, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    R = 20
+
+    def time_sigma(xx, yy, kind):
+        for _ in range(3):
+            g.sigma_device(xx.data_ptr(), yy.data_ptr(), kind)
+        a, b = ev(), ev()
+        torch.cuda.synchronize()
+        a.record(stream)
+        for _ in range(R):
+            g.sigma_device(xx.data_ptr(), yy.data_ptr(), kind)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / R
+
+    t_sig = time_sigma(x, y, 0)
+    # algorithmic bytes: values (none when recomputed) + int32 columns, per row int64
+    # start + int32 length, x and diag read once, y written once; the recomputing
+    # kernel also reads both strings of every determinant once (N * 16 B)
+    if prec64 == _capi.FP64:
+        b_sig = nnz_f * (8 + 4) + N * (8 + 4) + 3 * N * 8
+    elif prec64 == _capi.FP64_UPPER:  # each pair once; y is read-modify-written in L2
+        b_sig = nnz_u * (8 + 4) + N * (8 + 4) + 3 * N * 8
+    else:
+        b_sig = nnz_f * 4 + N * (8 + 4) + 3 * N * 8 + N * 16
+    peak, peak_kind = peaks()
+    sig_gbs = b_sig / (t_sig * 1e-3) / 1e9
+
+    # ---- sigma roofline, FP32 (the product path's dominant kernel) ----
+    g.build(precm)
+    x32 = x.float()
+    y32 = torch.empty_like(x32)
+    t_sig32 = time_sigma(x32, y32, 1)
+    full_m = precm == _capi.MIXED
+    b_sig32 = (nnz_f if full_m else nnz_u) * (4 + 4) + N * (8 + 4) + N * (4 + 4 + 8)
+    sig32_gbs = b_sig32 / (t_sig32 * 1e-3) / 1e9
 
     # ---- end to end through the public API: host dets in, energy + coefficients out ----
     pin = torch.empty((N, 4), dtype=torch.int64, pin_memory=True)
@@ -285,7 +372,8 @@ def main():
         a, b = ev(), ev()
         a.record(stream)
         g.set_dets(dets_pinned, 0, pin_diag.numpy())
-        e_api, c_api, _, _ = g.sparse_optimize(None, 1e-4, 1e-8, max_iter=DAV_MAX_ITER, precision=prec64)
+        e_api, c_api, _, _ = g.sparse_optimize(None, 1e-4, 1e-8, max_iter=DAV_MAX_ITER, precision=precm,
+                                               mode=_capi.MODE_MIXED, precond=precond)
         b.record(stream)
         torch.cuda.synchronize()
         e2e_ms.append(a.elapsed_time(b))
@@ -295,56 +383,10 @@ def main():
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e = float(et.item())
 
-    # ---- sigma roofline (x, y in the library's internal order) ----
-    g.build(prec64)
-    nnz_u, nnz_f = g.nnz()
-    x = torch.randn(N, dtype=torch.float64, device="cuda")
-    y = torch.empty_like(x)
-    torch.cuda.synchronize()
-    for _ in range(3):
-        g.sigma_device(x.data_ptr(), y.data_ptr(), 0)
-    R = 20
-    a, b = ev(), ev()
-    a.record(stream)
-    for _ in range(R):
-        g.sigma_device(x.data_ptr(), y.data_ptr(), 0)
-    b.record(stream)
-    torch.cuda.synchronize()
-    t_sig = a.elapsed_time(b) / R
-    # algorithmic bytes: values (none when recomputed) + int32 columns, per row int64
-    # start + int32 length, x and diag read once, y written once; the recomputing
-    # kernel also reads both strings of every determinant once (N * 16 B)
-    if prec64 == _capi.FP64:
-        b_sig = nnz_f * (8 + 4) + N * (8 + 4) + 3 * N * 8
-    elif prec64 == _capi.FP64_UPPER:  # each pair once; y is read-modify-written in L2
-        b_sig = nnz_u * (8 + 4) + N * (8 + 4) + 3 * N * 8
-    else:
-        b_sig = nnz_f * 4 + N * (8 + 4) + 3 * N * 8 + N * 16
-    peak, peak_kind = peaks()
-    sig_gbs = b_sig / (t_sig * 1e-3) / 1e9
-
-    # ---- mixed precision (FP32 sigma, FP64 dots / RR, closing FP64 sweeps) ----
-    a, b = ev(), ev()
-    precm = first_fitting([_capi.MIXED, _capi.MIXED_UPPER])
-    a.record(stream)
-    hs_m = g.build(precm)
-    rm = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=_capi.MODE_MIXED)
-    b.record(stream)
-    torch.cuda.synchronize()
-    ms_mixed = a.elapsed_time(b)
-    x32 = x.float()
-    y32 = torch.empty_like(x32)
-    for _ in range(3):
-        g.sigma_device(x32.data_ptr(), y32.data_ptr(), 1)
-    a, b = ev(), ev()
-    a.record(stream)
-    for _ in range(R):
-        g.sigma_device(x32.data_ptr(), y32.data_ptr(), 1)
-    b.record(stream)
-    torch.cuda.synchronize()
-    t_sig32 = a.elapsed_time(b) / R
-    b_sig32 = (nnz_f if precm == _capi.MIXED else nnz_u) * (4 + 4) + N * (8 + 4) + N * (4 + 4 + 8)
-
+    storage = {_capi.FP64: "FP64 both triangles", _capi.FP64_UPPER: "FP64 upper triangle",
+               _capi.COLS: "columns only, FP64 elements recomputed in sigma",
+               _capi.MIXED: "FP32 + FP32 remainder, both triangles",
+               _capi.MIXED_UPPER: "FP32 + FP32 remainder, upper triangle"}
     line = {
         "metric": METRIC,
         "value": N * world / (ms_max * 1e-3),
@@ -356,36 +398,44 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f32 sigma / f64 dots, Rayleigh-Ritz and closing sweeps",
         "data": "synthetic",
         "config": {"workload": f"hci n{cfg['n']} {cfg['nel']}a{cfg['nel']}b eps_var {cfg['eps']:g} seed 0",
                    "n_dets": int(N), "nnz_upper": int(nnz_u), "nnz_full": int(nnz_f),
-                   "step": "FP64 sparse-H build + plain DPR Davidson to E_var (tol 1e-4, etol 1e-8)",
-                   "fp64_storage": {_capi.FP64: "both triangles", _capi.FP64_UPPER: "upper triangle",
-                                    _capi.COLS: "columns, elements recomputed in sigma"}[prec64],
-                   "mixed_storage": None,
+                   "step": "mixed-precision sparse-H build + Davidson (FP32 sigma, learned preconditioner, "
+                           "closing FP64 sweeps) to E_var (tol 1e-4, etol 1e-8)",
+                   "precond": "learned (MLP, DPR fallback)" if model is not None else "DPR (no network for norb)",
+                   "storage": storage[precm], "fp64_storage": storage[prec64],
                    "l2": "CSR stream larger than L2 every step", "parallelism": f"replicas x{world}"},
         "e2e": {"value": N * world / (e2e * 1e-3), "unit": "dets/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": int(N * 40), "d2h_bytes_per_step": int(N * 8 + 8)},
-        "roofline": {"bound": "hbm", "kernel": {_capi.FP64: "k_spmv<FP64>", _capi.FP64_UPPER: "k_spmv_upper<FP64>",
-                                                _capi.COLS: "k_spmv_otf"}[prec64],
-                     "achieved": sig_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": sig_gbs / peak, "peak_kind": peak_kind, "traffic": None,
-                     "bytes_per_launch": int(b_sig), "ms_per_launch": t_sig},
-        "time_to_evar_ms": {"fp64_plain": ms_max, "mixed_dpr": ms_mixed,
-                            "mixed_storage": "both triangles" if precm == _capi.MIXED else "upper triangle",
-                            "dE_mixed_uHa": abs(float(rm.eigenvalues[0]) - e64) * 1e6,
-                            "fp64_iters": dstat["iters"], "mixed_iters": rm.stats["iters"],
-                            "mixed_fp64_sigmas": rm.stats["n_sigma_fp64"]},
-        "sigma": {"fp64_gbs": sig_gbs, "fp64_ms": t_sig, "fp32_gbs": b_sig32 / (t_sig32 * 1e-3) / 1e9,
-                  "fp32_ms": t_sig32, "fp32_frac": b_sig32 / (t_sig32 * 1e-3) / 1e9 / peak},
-        "h_build": {"elems_per_s": (nnz_u + N) / (hstat["ms_total"] * 1e-3), "ms": hstat["ms_total"],
-                    "gpu_ms_count": hstat["gpu_ms_count"], "gpu_ms_fill": hstat["gpu_ms_fill"],
-                    "candidates": hstat["candidates"]},
-        "davidson": {"iters": dstat["iters"], "n_sigma": dstat["n_sigma"], "ms": dstat["ms_total"],
-                     "ms_sigma": dstat["ms_sigma"], "energy": e64, "e_selection": e_sel},
+        "roofline": {"bound": "hbm",
+                     "kernel": "k_spmv<FP32>" if full_m else "k_spmv_upper<FP32>",
+                     "achieved": sig32_gbs, "peak": peak, "unit": "GB/s",
+                     "frac": sig32_gbs / peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_launch": int(b_sig32), "ms_per_launch": t_sig32},
+        "time_to_evar_ms": {"mixed_learned": ms_max, "fp64_plain": ms_plain, "mixed_dpr": ms_mixed_dpr,
+                            "mixed_dpr_iters": r_md.stats["iters"],
+                            "dE_mixed_dpr_vs_fp64_uHa": abs(float(r_md.eigenvalues[0]) - e64) * 1e6,
+                            "speedup_vs_fp64_plain": ms_plain / ms_max,
+                            "dE_vs_fp64_uHa": abs(e_m - e64) * 1e6,
+                            "mixed_iters": r_m.stats["iters"], "fp64_iters": r64.stats["iters"],
+                            "mixed_fp64_sigmas": r_m.stats["n_sigma_fp64"],
+                            "learned_fallbacks": r_m.stats["learned_fallbacks"],
+                            "mixed_build_ms": hs_m["ms_total"], "fp64_build_ms": hs64["ms_total"]},
+        "sigma": {"fp64_kernel": {_capi.FP64: "k_spmv<FP64>", _capi.FP64_UPPER: "k_spmv_upper<FP64>",
+                                  _capi.COLS: "k_spmv_otf"}[prec64],
+                  "fp64_gbs": sig_gbs, "fp64_ms": t_sig, "fp64_frac": sig_gbs / peak,
+                  "fp32_gbs": sig32_gbs, "fp32_ms": t_sig32, "fp32_frac": sig32_gbs / peak},
+        "h_build": {"elems_per_s": (nnz_u + N) / (hs64["ms_total"] * 1e-3), "ms": hs64["ms_total"],
+                    "gpu_ms_count": hs64["gpu_ms_count"], "gpu_ms_fill": hs64["gpu_ms_fill"],
+                    "candidates": hs64["candidates"]},
+        "davidson": {"energy_mixed": e_m, "energy_fp64": e64, "e_selection": e_sel,
+                     "mixed_ms": r_m.stats["ms_total"], "mixed_ms_sigma": r_m.stats["ms_sigma"],
+                     "fp64_ms": r64.stats["ms_total"], "fp64_ms_sigma": r64.stats["ms_sigma"]},
         "clocks": clk,
-        "gpu_launches": None,
+        "gpu_launches": launches_per_step * args.steps if launches_per_step is not None else None,
+        "gpu_launches_per_step": launches_per_step,
     }
     if rank == 0 and not args.no_cpu:
         s = cpu_sample(ints, dets, diag, vlog)

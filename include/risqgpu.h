@@ -244,7 +244,9 @@ RISQGPU_API int risqgpu_ham_off_diag(risqgpu_t* h, const uint64_t* d1, const uin
 
 /* Learned preconditioner (no counterpart in the reference, which has DPR only):
  * an MLP (2n+2) -> hidden -> hidden -> 1 (ReLU) gives each determinant a factor
- * f = clamp(exp(out), 0.25, 4) applied to its DPR step r_i / (lambda - H_ii).
+ * f = clamp(exp((out(x) + out(x~)) / 2), 0.25, 4), x~ being the features with the
+ * alpha and beta occupations exchanged (the factor is spin-flip symmetric, like
+ * H_ii), applied to its DPR step r_i / (lambda - H_ii).
  * Features: 2n occupations as +1/-1 (alpha orbitals, then beta), then
  * (H_ii - E - mu_e) * s_e and (sum of occupied h_pp - mu_h) * s_h with
  * feat_norm = {mu_e, s_e, mu_h, s_h} (NULL = {0, 1, 0, 1}).  Weights are row-major
@@ -258,11 +260,20 @@ RISQGPU_API int risqgpu_set_precond_mlp(risqgpu_t* h, int n_in, int hidden, cons
  * order (N floats).  For checking the network against a CPU evaluation. */
 RISQGPU_API int risqgpu_precond_factors(risqgpu_t* h, double energy, float* out);
 
+/* Second-order (Epstein-Nesbet) self-energy of every determinant at energy E over
+ * the stored matrix, caller order: out[i] = -sum_{j != i} H_ij^2 / max(H_jj - E, gmin)
+ * (N doubles; gmin > 0 keeps the sum finite when E reaches a diagonal).  No
+ * counterpart in the reference: it gives the learned preconditioner its training
+ * target f_i = sqrt((H_ii - E) / (H_ii - E + out[i])) at the converged FP64
+ * Davidson energy.  Needs stored values (not RISQGPU_COLS). */
+RISQGPU_API int risqgpu_self_energy(risqgpu_t* h, double energy, double gmin, double* out);
+
 /* MLP training on the device (forward and backward kernels of this library, Adam).
  * params: packed FP32 [W1 (H x n_in), b1 (H), W2 (H x H), b2 (H), W3 (H), b3 (1)];
  * feats: B x n_in features (already normalised), target: B factors, weight: B
- * sample weights.  Loss L = sum_b w_b (exp(o_b) - t_b)^2 / sum_b w_b, with o the
- * network output computed from BF16-rounded weights.
+ * sample weights.  Loss in log space, L = sum_b w_b (o_b - log t_b)^2 / sum_b w_b,
+ * with o the network output computed from BF16-rounded weights (one spin order;
+ * targets must be finite and positive, else RISQGPU_ERR_INVALID).
  * risqgpu_mlp_grad: L and dL/dparams (FP32, straight through the rounding) for
  * one batch.  risqgpu_mlp_train: `epochs` passes of Adam (lr, betas 0.9/0.999)
  * over shuffled minibatches of `batch` rows; params updated in place; loss_hist

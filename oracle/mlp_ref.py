@@ -4,7 +4,8 @@ TEST INFRASTRUCTURE: checks the library's forward and backward CUDA kernels
 (risqgpu_mlp_grad, risqgpu_precond_factors).  The network has no counterpart in the
 reference crate; it follows the definition in include/risqgpu.h:
 o = W3 relu(W2 relu(W1 x + b1) + b2) + b3 with W1, W2, W3 rounded to BF16 (round to
-nearest even), factor = exp(o); loss L = sum_b w_b (exp(o_b) - t_b)^2 / sum_b w_b.
+nearest even), factor = clamp(exp((o(x) + o(x~)) / 2), 0.25, 4) with x~ the features with
+the alpha and beta occupations exchanged; loss L = sum_b w_b (o_b - log t_b)^2 / sum_b w_b.
 """
 from __future__ import annotations
 
@@ -50,9 +51,9 @@ def loss_and_grad(params, X, t, w, n_in, H):
     t = np.asarray(t, dtype=np.float64)
     w = np.asarray(w, dtype=np.float64)
     W = w.sum()
-    e = np.exp(o)
-    loss = np.sum(w * (e - t) ** 2) / W
-    do = 2.0 * w * (e - t) * e / W
+    d = o - np.log(t)
+    loss = np.sum(w * d ** 2) / W
+    do = 2.0 * w * d / W
     dW3 = do @ h2
     db3 = do.sum()
     dh2 = np.outer(do, W3r) * (h2 > 0)
@@ -65,6 +66,15 @@ def loss_and_grad(params, X, t, w, n_in, H):
     return loss, g
 
 
+def swap_spins(X, norb):
+    """Features with the alpha and beta occupation blocks exchanged."""
+    Xs = np.array(X, copy=True)
+    Xs[:, :norb], Xs[:, norb:2 * norb] = X[:, norb:2 * norb], X[:, :norb]
+    return Xs
+
+
 def factors(params, X, n_in, H):
-    o, _ = forward(params, X, n_in, H)
-    return np.clip(np.exp(o), 0.25, 4.0)
+    norb = (n_in - 2) // 2
+    o1, _ = forward(params, X, n_in, H)
+    o2, _ = forward(params, swap_spins(X, norb), n_in, H)
+    return np.clip(np.exp(0.5 * (o1 + o2)), 0.25, 4.0)

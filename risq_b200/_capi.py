@@ -92,6 +92,7 @@ SIGNATURES = [
     ("risqgpu_ham_off_diag", C.c_int, [_handle, _u64p, _u64p, C.c_size_t, _dp]),
     ("risqgpu_set_precond_mlp", C.c_int, [_handle, C.c_int, C.c_int, _fp, _fp, _fp, _fp, _fp, _fp, _fp]),
     ("risqgpu_precond_factors", C.c_int, [_handle, C.c_double, _fp]),
+    ("risqgpu_self_energy", C.c_int, [_handle, C.c_double, C.c_double, _dp]),
     ("risqgpu_mlp_grad", C.c_int, [C.c_int, C.c_int, C.c_int, _fp, _fp, _fp, _fp, C.c_int64, _fp, _fp]),
     ("risqgpu_mlp_train", C.c_int, [C.c_int, C.c_int, C.c_int, _fp, _fp, _fp, _fp, C.c_int64, C.c_int, C.c_int,
                                     C.c_float, C.c_uint64, _fp]),

@@ -761,6 +761,13 @@ int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats*
         size_t need = (size_t)cap * (4 + vb) + ((size_t)64 << 20);
         size_t fr = 0, tot = 0;
         RQ_CUDA(h, cudaMemGetInfo(&fr, &tot));
+        // the current column and value arrays are released before the new ones are made
+        size_t held = 0;
+        if (h->d_cols) held += h->cap * sizeof(int32_t);
+        if (h->d_val64) held += h->cap * sizeof(double);
+        if (h->d_val32) held += h->cap * sizeof(float);
+        if (h->d_val_lo) held += h->cap * sizeof(float);
+        fr += held;
         if (need > fr) {
             h->err = "sparse H needs " + std::to_string(need >> 20) + " MiB, " + std::to_string(fr >> 20) +
                      " MiB free";
@@ -771,10 +778,10 @@ int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats*
         }
     }
     h->cap = (size_t)cap;
-    RQ_TRY(dalloc(h, h->d_cols, cap));
     dfree(h->d_val64);
     dfree(h->d_val32);
     dfree(h->d_val_lo);
+    RQ_TRY(dalloc(h, h->d_cols, cap));
     if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, cap));
     else if (precision != RISQGPU_COLS) RQ_TRY(dalloc(h, h->d_val32, cap));
     if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, cap));

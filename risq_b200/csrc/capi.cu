@@ -202,4 +202,10 @@ int risqgpu_precond_factors(risqgpu_t* h, double energy, float* out) {
     return precond_factors_impl(h, energy, out);
 }
 
+int risqgpu_self_energy(risqgpu_t* h, double energy, double gmin, double* out) {
+    if (!h || !out) return RISQGPU_ERR_INVALID;
+    DeviceGuard g(h->device);
+    return self_energy_impl(h, energy, gmin, out);
+}
+
 }  // extern "C"

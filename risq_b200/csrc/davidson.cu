@@ -387,11 +387,13 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
         RQ_CUDA(h, cudaMemcpyAsync(wk.small, hostsmall.data(), sizeof(double) * (dim * nr + nr), cudaMemcpyHostToDevice,
                                    h->stream));
         // learned scaling: refresh the per-determinant factors when the energy used in
-        // their features moved by more than 10 mHa; fall back to plain DPR for an
-        // iteration whenever the residual stalled (no new minimum in the last 3 iterations)
+        // their features moved by more than 0.1 Ha (the network is trained on features
+        // at the Ritz values of whole trajectories, so coarse refreshes suffice); fall
+        // back to plain DPR for an iteration whenever the residual stalled (no new
+        // minimum in the last 3 iterations)
         const float* fs = nullptr;
         if (fscale) {
-            if (std::isnan(e_feat) || std::fabs(w[0] - e_feat) > 1e-2) {
+            if (std::isnan(e_feat) || std::fabs(w[0] - e_feat) > 0.1) {
                 e_feat = w[0];
                 RQ_TRY(mlp_scale_impl(h, e_feat, fscale));
             }

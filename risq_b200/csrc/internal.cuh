@@ -188,5 +188,6 @@ int set_mlp_impl(risqgpu* h, int n_in, int hidden, const float* w1, const float*
                  const float* b2, const float* w3, const float* b3, const float* feat_norm);
 void free_mlp(risqgpu* h);
 int precond_factors_impl(risqgpu* h, double energy, float* out);
+int self_energy_impl(risqgpu* h, double energy, double gmin, double* out);
 
 }  // namespace risq

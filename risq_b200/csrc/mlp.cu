@@ -1,7 +1,8 @@
 // Learned diagonal-preconditioner correction: per-determinant inference.
 //
 // The network maps determinant features to a multiplicative correction of the
-// DPR step r_i / (lambda - H_ii): f_i = clamp(exp(MLP(x_i)), 0.25, 4).
+// DPR step r_i / (lambda - H_ii): f_i = clamp(exp((MLP(x_i) + MLP(x~_i)) / 2), 0.25, 4),
+// x~_i being the features with the alpha and beta occupations exchanged.
 // Features x_i (2n + 2 values, n = orbitals): occupation of each alpha orbital
 // then each beta orbital as +1 / -1, (H_ii - E - mu_e) * s_e, and
 // (sum of h_pp over the occupied spin-orbitals - mu_h) * s_h, where (mu_e, s_e,
@@ -36,7 +37,45 @@ uint16_t f_to_bf16(float f) {  // round to nearest even
 
 constexpr int HMAX = 128;
 
-// One thread per determinant; all weights staged in shared memory as FP32.
+// Network output o for one spin order: occupations of `a` fill inputs 0..n-1 and
+// those of `b` inputs n..2n-1.  W1, W2, W3, B1, B2 in shared memory (FP32 copies of
+// the BF16 weights).
+template <int W>
+__device__ __forceinline__ float mlp_out(const uint64_t (&a)[W], const uint64_t (&b)[W], int norb, int n_in,
+                                         int hidden, float dE, float sum_h, const float* W1, const float* B1,
+                                         const float* W2, const float* B2, const float* W3, float bias3) {
+    float hid[HMAX];
+#pragma unroll
+    for (int j = 0; j < HMAX; j++) {
+        if (j < hidden) {
+            const float* wr = W1 + j * n_in;
+            float s = B1[j];
+            for (int o = 0; o < norb; o++) {
+                s += wr[o] * (((a[o >> 6] >> (o & 63)) & 1ull) ? 1.f : -1.f);
+                s += wr[norb + o] * (((b[o >> 6] >> (o & 63)) & 1ull) ? 1.f : -1.f);
+            }
+            s += wr[2 * norb] * dE + wr[2 * norb + 1] * sum_h;
+            hid[j] = fmaxf(s, 0.f);
+        } else {
+            hid[j] = 0.f;
+        }
+    }
+    float o3 = bias3;
+    for (int j2 = 0; j2 < hidden; j2++) {
+        const float* wr = W2 + j2 * hidden;
+        float s = B2[j2];
+#pragma unroll
+        for (int j = 0; j < HMAX; j++) s += wr[j < hidden ? j : 0] * (j < hidden ? hid[j] : 0.f);
+        o3 += W3[j2] * fmaxf(s, 0.f);
+    }
+    return o3;
+}
+
+// One thread per determinant; all weights staged in shared memory as FP32.  The
+// factor is symmetric under the alpha <-> beta exchange, as the Hamiltonian is:
+// f = clamp(exp((o(alpha, beta) + o(beta, alpha)) / 2), 0.25, 4), so a determinant
+// and its spin-flipped partner get the same factor and the correction vector keeps
+// the spin-flip symmetry of the start vectors.
 template <int W>
 __global__ void __launch_bounds__(128) k_mlp_scale(const uint64_t* __restrict__ up, const uint64_t* __restrict__ dn,
                                                    const double* __restrict__ diag, int64_t N, int norb,
@@ -75,31 +114,9 @@ __global__ void __launch_bounds__(128) k_mlp_scale(const uint64_t* __restrict__ 
         }
         const float dE = ((float)(diag[p] - energy) - fnorm.x) * fnorm.y;
         sum_h = (sum_h - fnorm.z) * fnorm.w;
-        float hid[HMAX];
-#pragma unroll
-        for (int j = 0; j < HMAX; j++) {
-            if (j < hidden) {
-                const float* wr = W1 + j * n_in;
-                float s = B1[j];
-                for (int o = 0; o < norb; o++) {
-                    s += wr[o] * (((a[o >> 6] >> (o & 63)) & 1ull) ? 1.f : -1.f);
-                    s += wr[norb + o] * (((b[o >> 6] >> (o & 63)) & 1ull) ? 1.f : -1.f);
-                }
-                s += wr[2 * norb] * dE + wr[2 * norb + 1] * sum_h;
-                hid[j] = fmaxf(s, 0.f);
-            } else {
-                hid[j] = 0.f;
-            }
-        }
-        float o3 = bias3;
-        for (int j2 = 0; j2 < hidden; j2++) {
-            const float* wr = W2 + j2 * hidden;
-            float s = B2[j2];
-#pragma unroll
-            for (int j = 0; j < HMAX; j++) s += wr[j < hidden ? j : 0] * (j < hidden ? hid[j] : 0.f);
-            o3 += W3[j2] * fmaxf(s, 0.f);
-        }
-        float f = __expf(o3);
+        const float o_ab = mlp_out<W>(a, b, norb, n_in, hidden, dE, sum_h, W1, B1, W2, B2, W3, bias3);
+        const float o_ba = mlp_out<W>(b, a, norb, n_in, hidden, dE, sum_h, W1, B1, W2, B2, W3, bias3);
+        float f = __expf(0.5f * (o_ab + o_ba));
         out[p] = fminf(fmaxf(f, 0.25f), 4.0f);
     }
 }

@@ -3,7 +3,8 @@
 // Network (same as the inference kernel in mlp.cu): o = W3 relu(W2 relu(W1 x + b1)
 // + b2) + b3 with the weight matrices rounded to BF16 (round to nearest even) and
 // FP32 accumulation; factor = exp(o).  Loss over a batch of B rows with sample
-// weights w: L = sum_b w_b (exp(o_b) - t_b)^2 / sum_b w_b.  Gradients flow
+// weights w, in log space: L = sum_b w_b (o_b - log t_b)^2 / sum_b w_b (targets
+// t_b > 0 are factors, so the loss weighs halving and doubling alike).  Gradients flow
 // straight through the BF16 rounding into the FP32 master weights, which Adam
 // updates.  Every reduction runs in a fixed order, so training is reproducible.
 //
@@ -103,13 +104,12 @@ __global__ void __launch_bounds__(128) k_forward(const float* __restrict__ X, in
     }
 }
 
-// dL/do and the loss terms: do_b = 2 w_b (e^o - t) e^o / W
+// dL/do and the loss terms: do_b = 2 w_b (o_b - log t_b) / W
 __global__ void k_out_grad(const float* __restrict__ o, const float* __restrict__ t, const float* __restrict__ w,
                            int64_t B, float inv_w, float* __restrict__ dout, float* __restrict__ lterm) {
     for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < B; b += (int64_t)gridDim.x * blockDim.x) {
-        const float e = expf(o[b]);
-        const float d = e - t[b];
-        dout[b] = 2.f * w[b] * d * e * inv_w;
+        const float d = o[b] - logf(t[b]);
+        dout[b] = 2.f * w[b] * d * inv_w;
         lterm[b] = w[b] * d * d * inv_w;
     }
 }
@@ -301,6 +301,13 @@ struct DevScope {
     }
 };
 
+// targets are factors: the log-space loss needs every one finite and positive
+bool targets_ok(const float* t, int64_t B) {
+    for (int64_t b = 0; b < B; b++)
+        if (!(t[b] > 0.f) || !std::isfinite(t[b])) return false;
+    return true;
+}
+
 }  // namespace
 
 }  // namespace risq
@@ -310,6 +317,7 @@ using namespace risq;
 extern "C" int risqgpu_mlp_grad(int device, int n_in, int hidden, const float* params, const float* feats,
                                 const float* target, const float* weight, int64_t B, float* loss, float* grad) {
     if (!params || !feats || !target || !weight || !loss || !grad || B < 1) return RISQGPU_ERR_INVALID;
+    if (!targets_ok(target, B)) return RISQGPU_ERR_INVALID;
     RQ_TRY(check_dims(n_in, hidden));
     DevScope ds(device);
     Trainer T(n_in, hidden, B);
@@ -334,6 +342,7 @@ extern "C" int risqgpu_mlp_train(int device, int n_in, int hidden, float* params
                                  const float* target, const float* weight, int64_t B, int epochs, int batch,
                                  float lr, uint64_t seed, float* loss_hist) {
     if (!params || !feats || !target || !weight || B < 1 || epochs < 1 || batch < 1) return RISQGPU_ERR_INVALID;
+    if (!targets_ok(target, B)) return RISQGPU_ERR_INVALID;
     RQ_TRY(check_dims(n_in, hidden));
     DevScope ds(device);
     const int64_t bs = std::min<int64_t>(batch, B);

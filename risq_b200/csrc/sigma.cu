@@ -200,6 +200,43 @@ __global__ void k_permute_out(const double* __restrict__ yi, const int32_t* __re
         y[orig[p]] = yi[p];
 }
 
+// Second-order self-energy of every determinant over the stored matrix:
+// S_i = -sum_{j != i} H_ij^2 / max(H_jj - E, gmin).  VK as in k_spmv (0 FP64 values,
+// 1 FP32, 2 FP32 + remainder).  Full rows: one warp per row, private sum.  Upper
+// triangle: each stored pair adds to both rows (atomics; `out` zeroed first).
+template <int VK>
+__global__ void __launch_bounds__(256) k_self_energy(int64_t N, const int64_t* __restrict__ row_start,
+                                                     const int32_t* __restrict__ row_len,
+                                                     const int32_t* __restrict__ cols, const double* __restrict__ v64,
+                                                     const float* __restrict__ v32, const float* __restrict__ vlo,
+                                                     const double* __restrict__ diag, double energy, double gmin,
+                                                     int upper, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t p = warp; p < N; p += nwarps) {
+        const int64_t s = row_start[p];
+        const int len = row_len[p];
+        const double gp = fmax(diag[p] - energy, gmin);
+        double acc = 0.0;
+        for (int k = lane; k < len; k += 32) {
+            const int c = cols[s + k];
+            double v;
+            if constexpr (VK == 0) v = v64[s + k];
+            else if constexpr (VK == 2) v = (double)v32[s + k] + (double)vlo[s + k];
+            else v = (double)v32[s + k];
+            const double v2 = v * v;
+            acc += v2 / fmax(diag[c] - energy, gmin);
+            if (upper) atomicAdd(out + c, -v2 / gp);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) {
+            if (upper) atomicAdd(out + p, -acc);
+            else out[p] = -acc;
+        }
+    }
+}
+
 }  // namespace
 
 int spmv_grid(risqgpu* h) {
@@ -276,6 +313,36 @@ int sigma_host(risqgpu* h, const double* x, double* y, int nvec) {
     }
     RQ_TRY(sync(h, "sigma_host"));
     dfree(dx); dfree(dxi); dfree(dyi);
+    return RISQGPU_OK;
+}
+
+int self_energy_impl(risqgpu* h, double energy, double gmin, double* out) {
+    if (!h->built) { h->err = "self energy before build"; return RISQGPU_ERR_INVALID; }
+    if (h->precision == RISQGPU_COLS) { h->err = "self energy needs stored values (not COLS)"; return RISQGPU_ERR_INVALID; }
+    if (!(gmin > 0.0)) { h->err = "gmin must be positive"; return RISQGPU_ERR_INVALID; }
+    const int64_t n = (int64_t)h->N;
+    double *si = nullptr, *sc = nullptr;
+    RQ_TRY(dalloc(h, si, n));
+    RQ_TRY(dalloc(h, sc, n));
+    RQ_CUDA(h, cudaMemsetAsync(si, 0, sizeof(double) * n, h->stream));
+    const int grid = spmv_grid(h);
+    const int up = h->upper ? 1 : 0;
+    if (h->precision == RISQGPU_FP64)
+        k_self_energy<0><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, h->d_val64, nullptr,
+                                                      nullptr, h->d_diag, energy, gmin, up, si);
+    else if (h->precision == RISQGPU_MIXED)
+        k_self_energy<2><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr, h->d_val32,
+                                                      h->d_val_lo, h->d_diag, energy, gmin, up, si);
+    else
+        k_self_energy<1><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr, h->d_val32,
+                                                      nullptr, h->d_diag, energy, gmin, up, si);
+    RQ_TRY(check_launch(h, "self energy"));
+    int g = std::max(1, (int)std::min<int64_t>((n + 255) / 256, 148 * 16));
+    k_permute_out<<<g, 256, 0, h->stream>>>(si, h->d_orig, n, sc);
+    RQ_CUDA(h, cudaMemcpyAsync(out, sc, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "self energy"));
+    dfree(si);
+    dfree(sc);
     return RISQGPU_OK;
 }
 

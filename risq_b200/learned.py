@@ -5,13 +5,19 @@ The reference's Davidson uses DPR, t = r / (lambda - H_ii)
 each determinant a factor f in [0.25, 4] and the step becomes f * r / (lambda - H_ii);
 DPR stays the fallback whenever the residual stalls (risq_b200/csrc/davidson.cu).
 
-Training data are residual -> exact-correction pairs from FP64 Davidson runs:
-along a DPR trajectory (x_k, lambda_k, r_k) of a training system whose converged
-eigenvector x* is known, the ideal update is e = x* / (x*.x_k) - x_k; the DPR step is
-t = r_k / (lambda_k - H_ii); the target factor of determinant i is
-e_i / (a t_i), a = (e.t) / (t.t), clipped to [0.25, 4], and the sample weight is
-(a t_i)^2, so that the weighted loss is the squared error of the corrected step.
-Training runs on the device with this library's forward / backward kernels.
+Target.  DPR replaces H - lambda by its diagonal.  The second-order (Epstein-Nesbet)
+resolvent keeps the couplings of each determinant to first order:
+1 / (E - H_ii - S_i) with S_i = sum_j H_ij^2 / (E - H_jj) (risqgpu_self_energy).  The
+target factor of determinant i is f_i = sqrt((H_ii - E) / (H_ii - E + |S_i|)),
+clipped to [0.25, 4], at E = the converged energy of an FP64 DPR Davidson run on a
+training system.  The network sees E only through the feature H_ii - E, and during a
+solve E is the current Ritz value, so every training system contributes the same
+targets under features taken at the Ritz values its own FP64 DPR trajectory visits:
+the network learns the factor that suits the converged state from where the solver
+stands.  Inference averages the network over the determinant and its spin-flipped
+partner (alpha and beta occupations exchanged), so the factors keep the spin-flip
+symmetry of the Hamiltonian.  Training runs on the device with this library's
+forward / backward kernels (log-space squared error).
 
 Features (the inference kernel computes the same, mlp.cu): 2n occupations as +1/-1
 (alpha orbitals, then beta), (H_ii - E - mu_e) * s_e and
@@ -169,49 +175,39 @@ def dpr_trajectory(sigma, diag, tol=1e-4, etol=1e-8, max_iter=1000, record=None)
     return lam, x, max_iter
 
 
-def correction_samples(gpu, dets, diag, ints, per_iter=2000, rng=None, max_iter=1000):
-    """Residual -> exact-correction samples of one training system (FP64 Davidson)."""
+def self_energy(gpu, energy, gmin=1e-3):
+    """S_i = -sum_j H_ij^2 / max(H_jj - E, gmin) over the built matrix (risqgpu_self_energy)."""
+    out = np.zeros(gpu.n)
+    A.check(A.lib().risqgpu_self_energy(gpu._h, float(energy), float(gmin), A.ptr(out, A._dp)), gpu._h)
+    return out
+
+
+def target_factors(diag, S, energy):
+    """f_i = sqrt((H_ii - E) / (H_ii - E + S_i)) clipped to [0.25, 4] (S_i <= 0); 1 where
+    H_ii <= E.  The denominator is held at >= (H_ii - E) / 16, the clip's upper end."""
+    gap = np.asarray(diag, dtype=np.float64) - energy
+    with np.errstate(divide="ignore", invalid="ignore"):
+        den = np.maximum(gap + S, gap / 16.0)
+        f = np.sqrt(gap / den)
+    return np.where(gap > 0, np.clip(f, 0.25, 4.0), 1.0).astype(np.float32)
+
+
+def training_samples(gpu, dets, diag, ints, n_energies=12, per_energy=50000, rng=None, max_iter=2000):
+    """(features, targets, weights) of one training system with a built FP64 matrix."""
     rng = rng or np.random.default_rng(0)
-    sigma = gpu.matrix_vector_prod
-    # converged reference eigenvector
-    lam_star, x_star, _ = dpr_trajectory(sigma, diag, tol=1e-7, etol=1e-12, max_iter=max_iter)
-    x_star = x_star / np.linalg.norm(x_star)
-    feats, targets, weights = [], [], []
-
-    def record(k, lam, x, r):
-        nx = np.linalg.norm(x)
-        x = x / nx
-        r = r / nx
-        ov = x_star @ x
-        if abs(ov) < 0.3:
-            return
-        e = x_star / ov - x
-        t = r / (lam - diag)
-        tt = t @ t
-        if tt <= 0:
-            return
-        a = (e @ t) / tt
-        if a == 0:
-            return
-        at = a * t
-        with np.errstate(divide="ignore", invalid="ignore"):
-            f = np.where(np.abs(at) > 0, e / at, 1.0)
-        f = np.clip(np.nan_to_num(f, nan=1.0, posinf=4.0, neginf=0.25), 0.25, 4.0)
-        w = at * at
-        s = w.sum()
-        if not s > 0:
-            return
-        m = min(per_iter, len(diag))
-        idx = rng.choice(len(diag), size=m, replace=False, p=w / s)
-        raw = raw_features(dets[idx], diag[idx], lam, ints)
-        feats.append(raw)
-        targets.append(f[idx].astype(np.float32))
-        weights.append(np.ones(m, dtype=np.float32))
-
-    dpr_trajectory(sigma, diag, tol=1e-4, etol=1e-8, max_iter=max_iter, record=record)
-    if not feats:
-        return None
-    return np.concatenate(feats), np.concatenate(targets), np.concatenate(weights)
+    lams = []
+    lam_star, _, iters = dpr_trajectory(gpu.matrix_vector_prod, diag, tol=1e-4, etol=1e-8, max_iter=max_iter,
+                                        record=lambda k, lam, x, r: lams.append(float(lam)))
+    f = target_factors(diag, self_energy(gpu, lam_star), lam_star)
+    pick = np.asarray(lams)[np.unique(np.linspace(0, len(lams) - 1, n_energies).astype(int))]
+    N = len(diag)
+    feats, targets = [], []
+    for E in pick:
+        idx = np.sort(rng.choice(N, size=min(per_energy, N), replace=False))
+        feats.append(raw_features(dets[idx], diag[idx], E, ints))
+        targets.append(f[idx])
+    F = np.concatenate(feats)
+    return F, np.concatenate(targets), np.ones(len(F), dtype=np.float32), dict(energy=lam_star, iters=iters)
 
 
 def grad(model: PrecondMLP, feats, target, weight, device=0):
@@ -241,9 +237,10 @@ def train(model: PrecondMLP, feats, target, weight, epochs=20, batch=4096, lr=1e
     return hist
 
 
-def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, device=0, per_iter=2000, log=print):
-    """systems: list of (ints, dets, diag).  Builds the samples, fits the feature
-    normalisation and trains a fresh network."""
+def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, device=0, n_energies=12,
+                       per_energy=50000, log=print):
+    """systems: list of (ints, dets, diag).  Builds the samples (FP64 matrix and FP64
+    DPR Davidson per system), fits the feature normalisation and trains a fresh network."""
     from .gpu import GpuHam
     F, T, Wt = [], [], []
     rng = np.random.default_rng(seed)
@@ -251,11 +248,11 @@ def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, de
         with GpuHam(ints, device) as g:
             g.set_dets(dets, 0, diag)
             g.build(A.FP64)
-            smp = correction_samples(g, dets, diag, ints, per_iter=per_iter, rng=rng)
-        if smp is None:
-            continue
-        F.append(smp[0]); T.append(smp[1]); Wt.append(smp[2])
-        log(f"# training system {k}: {len(dets)} dets, {len(smp[1])} samples")
+            f, t, w, info = training_samples(g, dets, diag, ints, n_energies=n_energies, per_energy=per_energy,
+                                             rng=rng)
+        F.append(f); T.append(t); Wt.append(w)
+        log(f"# training system {k}: {len(dets)} dets, E = {info['energy']:.8f} after {info['iters']} DPR "
+            f"iterations, {len(t)} samples, target factor median {np.median(t):.3f}")
     raw = np.concatenate(F)
     n2 = raw.shape[1] - 2
     mu_e, sd_e = float(raw[:, n2].mean()), float(raw[:, n2].std() + 1e-6)
@@ -268,5 +265,5 @@ def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, de
 
 
 __all__ = ["PrecondMLP", "install", "device_factors", "raw_features", "normalise", "dpr_trajectory",
-           "correction_samples", "grad", "train", "train_from_systems", "load_default", "default_model_path",
-           "dets_to_ints"]
+           "self_energy", "target_factors", "training_samples", "grad", "train", "train_from_systems",
+           "load_default", "default_model_path", "dets_to_ints"]

@@ -5,8 +5,9 @@
 
 Training systems: seeded synthetic integrals (risq_b200.fcidump.synthetic_integrals)
 with the given orbitals / electrons, their HCI determinant sets made by this
-library's device variational stage, and residual -> exact-correction samples from
-FP64 Davidson on each (risq_b200.learned).  The network is then evaluated on seed 0
+library's device variational stage, and per-determinant target factors from the
+second-order self-energy at the converged FP64 Davidson energy, with features taken
+at the Ritz values of the FP64 DPR trajectory (risq_b200.learned).  The network is then evaluated on seed 0
 (held out): Davidson iterations and time with and without it.
 """
 from __future__ import annotations
@@ -35,7 +36,8 @@ def main():
     ap.add_argument("--eps", type=float, default=1e-3)
     ap.add_argument("--seeds", default="1-8")
     ap.add_argument("--epochs", type=int, default=30)
-    ap.add_argument("--per-iter", type=int, default=2000)
+    ap.add_argument("--n-energies", type=int, default=12)
+    ap.add_argument("--per-energy", type=int, default=50000)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default=None)
     ap.add_argument("--device", type=int, default=0)
@@ -49,7 +51,8 @@ def main():
         print(f"# seed {s}: {len(dets)} dets, E = {e:.8f}", flush=True)
         systems.append((ints, dets, diag))
     model, hist = learned.train_from_systems(systems, args.norb, epochs=args.epochs, lr=args.lr,
-                                             per_iter=args.per_iter, device=args.device)
+                                             n_energies=args.n_energies, per_energy=args.per_energy,
+                                             device=args.device)
     print("# loss per epoch:", " ".join(f"{x:.4g}" for x in hist), flush=True)
     out = args.out or learned.default_model_path(args.norb)
     model.save(out)

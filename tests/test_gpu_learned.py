@@ -77,3 +77,43 @@ def test_learned_preconditioner_gain_on_held_out_system():
     assert base.converged and lr.converged
     assert abs(lr.eigenvalues[0] - base.eigenvalues[0]) < 1e-6
     assert lr.stats["iters"] < base.stats["iters"]
+
+
+def _self_energy_ref(rp, cols, vals, diag, E, gmin):
+    """numpy: S_i = -sum_{j != i} H_ij^2 / max(H_jj - E, gmin) from the stored upper triangle."""
+    N = len(diag)
+    rows = np.repeat(np.arange(N), np.diff(rp))
+    g = np.maximum(diag - E, gmin)
+    v2 = vals * vals
+    S = np.zeros(N)
+    np.add.at(S, rows, -v2 / g[cols])
+    np.add.at(S, cols, -v2 / g[rows])
+    return S
+
+
+@pytest.mark.parametrize("prec", [_capi.FP64, _capi.MIXED, _capi.FP64_UPPER])
+def test_self_energy_matches_numpy(prec):
+    ints, p = H.golden_system("be2")
+    _, dets, _, diag, _ = H.oracle_hci("be2")
+    E = float(diag.min()) - 0.05
+    with GpuHam(ints) as g:
+        g.set_dets(dets, 0, diag)
+        g.build(_capi.FP64)
+        rp, cols, vals, dg = g.export_upper()
+        g.build(prec)
+        S = learned.self_energy(g, E, 1e-3)
+    ref = _self_energy_ref(rp, cols, vals, dg, E, 1e-3)
+    # MIXED stores FP32 + FP32 remainder (about 2^-48 relative); sums run in another order
+    np.testing.assert_allclose(S, ref, rtol=1e-9, atol=1e-14)
+    f = learned.target_factors(dg, S, E)
+    assert np.all((f >= 0.25) & (f <= 4.0))
+
+
+def test_self_energy_rejects_columns_only_storage():
+    ints, p = H.golden_system("be2")
+    _, dets, _, diag, _ = H.oracle_hci("be2")
+    with GpuHam(ints) as g:
+        g.set_dets(dets, 0, diag)
+        g.build(_capi.COLS)
+        with pytest.raises(_capi.RisqGpuError):
+            learned.self_energy(g, -10.0)

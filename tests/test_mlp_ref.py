@@ -48,3 +48,30 @@ def test_features_layout():
     assert abs(f[0, 13] - (hpp[0] + hpp[1] + hpp[2] + hpp[0] + hpp[1] + hpp[3])) < 1e-5
     g = normalise(f, np.array([1.0, 2.0, 0.0, 0.5], dtype=np.float32))
     assert g[0, 12] == 0.0 and abs(g[0, 13] - 0.5 * f[0, 13]) < 1e-6
+
+
+def test_reference_factors_are_spin_flip_symmetric():
+    norb, H = 5, 16
+    m = PrecondMLP.init(norb, hidden=H, seed=2)
+    rng = np.random.default_rng(3)
+    m.params = (m.params + 0.1 * rng.standard_normal(m.params.shape)).astype(np.float32)
+    X = rng.standard_normal((50, 2 * norb + 2)).astype(np.float32)
+    f = mlp_ref.factors(m.params, X, m.n_in, H)
+    fs = mlp_ref.factors(m.params, mlp_ref.swap_spins(X, norb), m.n_in, H)
+    np.testing.assert_array_equal(f, fs)
+    assert np.all((f >= 0.25) & (f <= 4.0))
+
+
+def test_target_factors():
+    from risq_b200.learned import target_factors
+    diag = np.array([-1.0, 0.0, 1.0, 1.0, 1.0, 3.0])
+    E = -1.0
+    # gap: 0 (-> 1), 1, 2, 2, 2, 4
+    S = np.array([-5.0, 0.0, -1.0, -1.9, -100.0, -3.0])
+    f = target_factors(diag, S, E)
+    assert f[0] == 1.0                      # H_ii <= E: no correction
+    assert f[1] == 1.0                      # no coupling: DPR
+    assert abs(f[2] - np.sqrt(2.0)) < 1e-6  # sqrt(gap / (gap - |S|))
+    assert abs(f[3] - 4.0) < 1e-6           # denominator held at gap / 16 -> clip end
+    assert f[4] == 4.0
+    assert abs(f[5] - 2.0) < 1e-6
