@@ -5,7 +5,9 @@ TEST INFRASTRUCTURE: checks the library's forward and backward CUDA kernels
 reference crate; it follows the definition in include/risqgpu.h:
 o = W3 relu(W2 relu(W1 x + b1) + b2) + b3 with W1, W2, W3 rounded to BF16 (round to
 nearest even), factor = clamp(exp((o(x) + o(x~)) / 2), 0.25, 4) with x~ the features with
-the alpha and beta occupations exchanged; loss L = sum_b w_b (o_b - log t_b)^2 / sum_b w_b.
+the alpha and beta occupations exchanged and the first layer's activations rounded to
+BF16 (inference); loss L = sum_b w_b (o_b - log t_b)^2 / sum_b w_b with FP32 activations
+(training).
 """
 from __future__ import annotations
 
@@ -34,12 +36,16 @@ def unpack(params, n_in, H):
     return W1, b1, W2, b2, W3, b3
 
 
-def forward(params, X, n_in, H):
+def forward(params, X, n_in, H, act_bf16=False):
+    """Network output.  act_bf16: round the first layer's activations to BF16, as
+    inference does (the trainer keeps them FP32)."""
     W1, b1, W2, b2, W3, b3 = unpack(params, n_in, H)
     W1r, W2r, W3r = (bf16_round(w).astype(np.float64) for w in (W1, W2, W3))
     X = np.asarray(X, dtype=np.float64)
     z1 = X @ W1r.T + b1
     h1 = np.maximum(z1, 0.0)
+    if act_bf16:
+        h1 = bf16_round(h1.astype(np.float32)).astype(np.float64)
     z2 = h1 @ W2r.T + b2
     h2 = np.maximum(z2, 0.0)
     o = h2 @ W3r + b3[0]
@@ -75,6 +81,6 @@ def swap_spins(X, norb):
 
 def factors(params, X, n_in, H):
     norb = (n_in - 2) // 2
-    o1, _ = forward(params, X, n_in, H)
-    o2, _ = forward(params, swap_spins(X, norb), n_in, H)
+    o1, _ = forward(params, X, n_in, H, act_bf16=True)
+    o2, _ = forward(params, swap_spins(X, norb), n_in, H, act_bf16=True)
     return np.clip(np.exp(0.5 * (o1 + o2)), 0.25, 4.0)

@@ -8,7 +8,9 @@
 // (sum of h_pp over the occupied spin-orbitals - mu_h) * s_h, where (mu_e, s_e,
 // mu_h, s_h) are the network's feature normalisation.  Layers
 // (2n+2) -> hidden -> hidden -> 1 with ReLU; weights are rounded to BF16 (round
-// to nearest even) on the device and every product accumulates in FP32.
+// to nearest even) on the device, every product accumulates in FP32, and the
+// first layer's activations are rounded to BF16 (they are the A operand of the
+// second layer's BF16 GEMM on the tensor-core path, mlp_tc.cu).
 // There is no counterpart in the reference (which only has DPR,
 // algorithms/davidson.rs:391-408); the reference's DPR is the fallback.
 #include <algorithm>
@@ -25,6 +27,12 @@ namespace risq {
 namespace {
 
 __device__ __forceinline__ float bf16_to_f(uint16_t u) { return __uint_as_float(((uint32_t)u) << 16); }
+
+__device__ __forceinline__ uint16_t f_to_bf16_dev(float f) {  // round to nearest even (finite values)
+    uint32_t u = __float_as_uint(f);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
 
 uint16_t f_to_bf16(float f) {  // round to nearest even
     uint32_t u;
@@ -55,7 +63,7 @@ __device__ __forceinline__ float mlp_out(const uint64_t (&a)[W], const uint64_t 
                 s += wr[norb + o] * (((b[o >> 6] >> (o & 63)) & 1ull) ? 1.f : -1.f);
             }
             s += wr[2 * norb] * dE + wr[2 * norb + 1] * sum_h;
-            hid[j] = fmaxf(s, 0.f);
+            hid[j] = bf16_to_f(f_to_bf16_dev(fmaxf(s, 0.f)));  // BF16 activations, as the tensor-core path
         } else {
             hid[j] = 0.f;
         }
@@ -161,8 +169,12 @@ int set_mlp_impl(risqgpu* h, int n_in, int hidden, const float* w1, const float*
     return RISQGPU_OK;
 }
 
+int mlp_scale_tc(risqgpu* h, double energy, float* out);
+
 int mlp_scale_impl(risqgpu* h, double energy, float* out) {
     if (!h->mlp.loaded) { h->err = "no MLP loaded"; return RISQGPU_ERR_INVALID; }
+    // hidden width 128 with 2n <= 128 runs on the tensor cores; other shapes on the CUDA cores
+    if (h->mlp.hidden == 128 && 2 * h->norb <= 128) return mlp_scale_tc(h, energy, out);
     const int hid = h->mlp.hidden, nin = h->mlp.n_in;
     size_t smem = sizeof(float) * ((size_t)hid * nin + (size_t)hid * hid + 3 * hid + h->norb);
     const int64_t N = (int64_t)h->N;

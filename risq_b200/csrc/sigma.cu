@@ -168,14 +168,25 @@ __global__ void __launch_bounds__(256) k_spmv_upper(int64_t N, const int64_t* __
         const X xp = x[p];
         X acc = 0;
         int k = lane;
-        for (; k + 32 < len; k += 64) {
+        // four independent element loads in flight per lane before the gathers and scatters
+        for (; k + 96 < len; k += 128) {
             const int c0 = __ldcs(cols + s + k), c1 = __ldcs(cols + s + k + 32);
+            const int c2 = __ldcs(cols + s + k + 64), c3 = __ldcs(cols + s + k + 96);
             X v0 = (X)__ldcs(vals + s + k), v1 = (X)__ldcs(vals + s + k + 32);
-            if constexpr (VLO) { v0 += (X)__ldcs(vlo + s + k); v1 += (X)__ldcs(vlo + s + k + 32); }
-            acc += v0 * __ldg(x + c0);
-            acc += v1 * __ldg(x + c1);
+            X v2 = (X)__ldcs(vals + s + k + 64), v3 = (X)__ldcs(vals + s + k + 96);
+            if constexpr (VLO) {
+                v0 += (X)__ldcs(vlo + s + k); v1 += (X)__ldcs(vlo + s + k + 32);
+                v2 += (X)__ldcs(vlo + s + k + 64); v3 += (X)__ldcs(vlo + s + k + 96);
+            }
+            const X x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
+            acc += v0 * x0;
+            acc += v1 * x1;
+            acc += v2 * x2;
+            acc += v3 * x3;
             atomicAdd(y + c0, v0 * xp);
             atomicAdd(y + c1, v1 * xp);
+            atomicAdd(y + c2, v2 * xp);
+            atomicAdd(y + c3, v3 * xp);
         }
         for (; k < len; k += 32) {
             const int c = __ldcs(cols + s + k);
