@@ -196,6 +196,9 @@ def main():
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--impl", default="risq_b200")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--storage", choices=["auto", "upper"], default="auto",
+                    help="auto: both triangles when they fit, else the upper triangle; upper: always the "
+                         "upper triangle (the reference's SparseMatUpperTri layout)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -251,7 +254,8 @@ def main():
 
     # product path storage: FP32 + FP32 remainder rows when both triangles fit, else the
     # upper triangle (the reference's SparseMatUpperTri layout)
-    precm = first_fitting([_capi.MIXED, _capi.MIXED_UPPER])
+    upper_only = args.storage == "upper"
+    precm = first_fitting([_capi.MIXED_UPPER] if upper_only else [_capi.MIXED, _capi.MIXED_UPPER])
 
     def product_step():
         hs = g.build(precm)
@@ -303,9 +307,9 @@ def main():
     ms_mixed_dpr = a.elapsed_time(b)
 
     # ---- plain FP64 GPU path on the same set: FP64 build + the reference's DPR Davidson ----
-    prec64 = first_fitting([_capi.FP64, _capi.FP64_UPPER, _capi.COLS])
+    prec64 = first_fitting([_capi.FP64_UPPER, _capi.COLS] if upper_only else [_capi.FP64, _capi.FP64_UPPER, _capi.COLS])
     plain_ms, plain = [], None
-    for i in range(1 + max(1, min(args.steps, 2))):
+    for i in range(2):
         a, b = ev(), ev()
         torch.cuda.synchronize()
         a.record(stream)
@@ -367,7 +371,7 @@ def main():
     pin_diag.numpy()[:] = diag
     dets_pinned = pin.numpy().view(np.uint64)
     e2e_ms = []
-    for i in range(max(1, min(args.steps, 3))):
+    for i in range(max(1, min(args.steps, 2))):
         torch.cuda.synchronize()
         a, b = ev(), ev()
         a.record(stream)

@@ -279,3 +279,37 @@ def test_upper_triangle_storage(name):
             g.davidson(1, None, 1e-4, 1e-8, 50, mode=_capi.MODE_MIXED)  # FP32 upper has no FP64 sigma
         with pytest.raises(_capi.RisqGpuError):
             g.set_dets(dets, len(dets), diag)  # no incremental extension of an upper build
+
+
+def test_upper_triangle_sigma_on_large_alpha_groups():
+    """The blocked upper-triangle sigma on a set whose alpha groups exceed both the
+    1024-column window and the 256-row work item (n20 8a8b, eps 1e-3): FP64 against
+    the both-triangle kernel (checked against the oracle above), FP32 and the FP32 +
+    remainder storage against the same reference."""
+    from risq_b200.fcidump import synthetic_integrals
+    ints = synthetic_integrals(20, 0)
+    with _gpu(ints) as g:
+        e, dets, c, diag, log = g.variational(8, 8, 1e-3, dav_max_iter=2000)
+        up = dets[:, 0]
+        _, counts = np.unique(up, return_counts=True)
+        assert counts.max() > 1024  # windows are split and groups span several work items
+        x = np.random.default_rng(3).standard_normal(len(dets))
+        g.set_dets(dets, 0, diag)
+        g.build(_capi.FP64)
+        ref = g.matrix_vector_prod(x)
+        scale = np.max(np.abs(ref))
+        g.build(_capi.FP64_UPPER)
+        y = g.matrix_vector_prod(x)
+        assert np.max(np.abs(y - ref)) <= 1e-12 * scale
+        g.build(_capi.MIXED_UPPER)
+        y = g.matrix_vector_prod(x)  # FP64 sigma over FP32 value + FP32 remainder
+        assert np.max(np.abs(y - ref)) <= 1e-11 * scale
+        import torch
+        perm_free = torch.tensor(x, dtype=torch.float32, device="cuda")  # FP32 sigma, internal order
+        y32 = torch.empty_like(perm_free)
+        g.build(_capi.FP32)
+        g.sigma_device(perm_free.data_ptr(), y32.data_ptr(), 1)
+        ref32 = y32.double().cpu().numpy()
+        g.build(_capi.FP32_UPPER)
+        g.sigma_device(perm_free.data_ptr(), y32.data_ptr(), 1)
+        assert np.max(np.abs(y32.double().cpu().numpy() - ref32)) <= 1e-5 * np.max(np.abs(ref32))
