@@ -172,6 +172,29 @@ __global__ void k_pa_start(const int64_t* __restrict__ off_e, int64_t G, int nup
         pa_start[g] = (int32_t)(g < G ? off_e[g * nup] : total);
 }
 
+// Hash of (alpha group, beta string) for the determinant table (splitmix64 finaliser).
+__device__ __forceinline__ uint64_t det_hash(uint32_t g, uint64_t beta) {
+    uint64_t h = beta * 0x9E3779B97F4A7C15ull ^ ((uint64_t)(g + 1) * 0xC2B2AE3D27D4EB4Full);
+    h ^= h >> 31;
+    h *= 0xBF58476D1CE4E5B9ull;
+    h ^= h >> 29;
+    return h;
+}
+
+// Insert every determinant (one-word strings) into the open-addressing table.
+__global__ void k_ht_insert(int64_t n, const int32_t* __restrict__ ga, const uint64_t* __restrict__ dn, int bits,
+                            int32_t* __restrict__ ht) {
+    const uint32_t mask = (1u << bits) - 1u;
+    for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
+        uint32_t slot = (uint32_t)(det_hash((uint32_t)ga[q], dn[q]) >> (64 - bits));
+        // the table has at least 2n slots, so an empty one is always found
+        for (uint32_t t = 0; t <= mask; t++) {
+            if (atomicCAS(ht + slot, -1, (int32_t)q) == -1) break;
+            slot = (slot + 1) & mask;
+        }
+    }
+}
+
 template <int W>
 struct SetView {
     const uint64_t* __restrict__ up;
@@ -188,6 +211,10 @@ struct SetView {
     const int32_t* __restrict__ pa_list;
     const int32_t* __restrict__ orig;
     int64_t nsh;
+    int norb;
+    // (alpha group, beta string) -> internal index, or null (two-word strings)
+    const int32_t* __restrict__ ht;
+    int ht_bits;
     // previous build (incremental extension)
     const int32_t* __restrict__ prev_inv_of_caller;  // caller -> previous internal (or null)
     const int64_t* __restrict__ prev_row_start;
@@ -217,7 +244,29 @@ struct SetView {
         for (int k = 0; k < W; k++) b.w[k] = __ldg(up_b + k * N + t);
         return b;
     }
+    // internal index of the determinant (alpha group g, beta string beta), or -1
+    __device__ __forceinline__ int find(int g, uint64_t beta) const {
+        const uint32_t mask = (1u << ht_bits) - 1u;
+        uint32_t slot = (uint32_t)(det_hash((uint32_t)g, beta) >> (64 - ht_bits));
+        for (uint32_t t = 0; t <= mask; t++) {
+            const int q = __ldg(ht + slot);
+            if (q < 0) return -1;
+            if (__ldg(ga + q) == g && __ldg(dn + q) == beta) return q;
+            slot = (slot + 1) & mask;
+        }
+        return -1;
+    }
 };
+
+// n-th (0-based) set bit of x; 64 if there is none
+__device__ __forceinline__ int nth_set_bit(uint64_t x, int n) {
+    for (int k = 0; k < n && x; k++) x &= x - 1;
+    return x ? __ffsll((long long)x) - 1 : 64;
+}
+
+// Alpha partner groups with more determinants than this are searched through the
+// determinant table rather than scanned.
+constexpr int LOOKUP_MIN_GROUP = 256;
 
 // Kinds of structural hits, evaluated in batches.
 enum HitKind : int { K_SING_B = 0, K_SING_A = 1, K_DOUB_B = 2, K_DOUB_A = 3, K_OPP = 4 };
@@ -369,18 +418,66 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
                 push(hit, d == 2, q, d == 2 ? K_SING_A : K_DOUB_A);
             }
         }
-        // (3) alpha single-partner groups: opposite-spin doubles
+        // (3) alpha single-partner groups: opposite-spin doubles.  A small partner group
+        // is scanned for beta strings one single excitation away; a large one (one-word
+        // strings) is probed in the determinant table with the single excitations of
+        // beta_p instead (n_beta x (norb - n_beta) lookups in place of |group| tests).
         {
             const int g = v.ga[p];
             const int ps = v.pa_start[g], pe = v.pa_start[g + 1];
+            // this row's occupied / virtual beta orbitals, k-th of each in lane k % 32, word k / 32
+            int occ0 = 64, occ1 = 64, vir0 = 64, vir1 = 64, n_occ = 0, n_vir = 0;
+            if constexpr (W == 1) {
+                if (v.ht) {
+                    const uint64_t all = v.norb >= 64 ? ~0ull : ((1ull << v.norb) - 1ull);
+                    const uint64_t bo = b.w[0], bv = ~b.w[0] & all;
+                    n_occ = __popcll(bo);
+                    n_vir = __popcll(bv);
+                    occ0 = nth_set_bit(bo, lane);
+                    occ1 = nth_set_bit(bo, lane + 32);
+                    vir0 = nth_set_bit(bv, lane);
+                    vir1 = nth_set_bit(bv, lane + 32);
+                }
+            }
             for (int c0 = ps; c0 < pe; c0 += 32) {
                 const int nvalid = min(32, pe - c0);
-                int gs = 0, gl = 0;
+                int gs = 0, gl = 0, g2 = -1;
+                bool probe = false;
                 if (lane < nvalid) {
-                    const int g2 = v.pa_list[c0 + lane];
+                    g2 = v.pa_list[c0 + lane];
                     gs = v.ga_start[g2];
                     // groups are ordered by index: a lower group holds only q < p
                     gl = (upper && g2 < g) ? 0 : v.ga_start[g2 + 1] - gs;
+                    if (W == 1 && v.ht && gl > LOOKUP_MIN_GROUP) {
+                        probe = true;
+                        gl = 0;
+                    }
+                }
+                // large groups: probe the table with the single excitations of beta_p
+                if constexpr (W == 1) {
+                    unsigned big = __ballot_sync(FULL, probe);
+                    while (big) {
+                        const int src = __ffs(big) - 1;
+                        big &= big - 1;
+                        const int gg = __shfl_sync(FULL, g2, src);
+                        const int total = n_occ * n_vir;
+                        for (int t0 = 0; t0 < total; t0 += 32) {
+                            const int idx = t0 + lane;
+                            bool hit = false;
+                            int q = -1;
+                            const int io = idx / max(n_vir, 1), iv = idx - io * max(n_vir, 1);
+                            // the requesting lane picks the word: shuffle both, select after
+                            const int o0 = __shfl_sync(FULL, occ0, io & 31), o1 = __shfl_sync(FULL, occ1, io & 31);
+                            const int v0 = __shfl_sync(FULL, vir0, iv & 31), v1 = __shfl_sync(FULL, vir1, iv & 31);
+                            const int oi = io < 32 ? o0 : o1, vi = iv < 32 ? v0 : v1;
+                            if (idx < total) {
+                                const uint64_t beta = b.w[0] ^ (1ull << oi) ^ (1ull << vi);
+                                q = v.find(gg, beta);
+                                hit = q >= 0 && (p_new || v.orig[q] >= v.nsh);
+                            }
+                            push(hit, false, q, K_OPP);
+                        }
+                    }
                 }
                 int incl = gl;
 #pragma unroll
@@ -696,6 +793,9 @@ SetView<W> make_view(risqgpu* h, bool with_prev, const int32_t* prev_inv_caller)
     v.ga = h->d_ga; v.ga_start = h->d_ga_start; v.gb = h->d_gb; v.gb_start = h->d_gb_start;
     v.order_b = h->d_order_b; v.pos_b = h->d_pos_b; v.pa_start = h->d_pa_start; v.pa_list = h->d_pa_list;
     v.orig = h->d_orig; v.nsh = (int64_t)h->nsh; v.inv = h->d_inv;
+    v.norb = h->norb;
+    v.ht = h->d_ht;
+    v.ht_bits = h->ht_bits;
     v.prev_inv_of_caller = with_prev ? prev_inv_caller : nullptr;
     v.prev_row_start = h->d_prev_row_start; v.prev_row_len = h->d_prev_row_len; v.prev_cols = h->d_prev_cols;
     v.prev_orig = h->d_prev_orig; v.prev_v64 = h->d_prev_val64; v.prev_v32 = h->d_prev_val32;
@@ -863,7 +963,8 @@ static void free_prev(risqgpu* h) {
 void free_dets(risqgpu* h) {
     dfree(h->d_up); dfree(h->d_dn); dfree(h->d_up_b); dfree(h->d_orig); dfree(h->d_inv); dfree(h->d_diag);
     dfree(h->d_ga); dfree(h->d_ga_start); dfree(h->d_gb); dfree(h->d_gb_start); dfree(h->d_order_b);
-    dfree(h->d_pos_b); dfree(h->d_pa_start); dfree(h->d_pa_list);
+    dfree(h->d_pos_b); dfree(h->d_pa_start); dfree(h->d_pa_list); dfree(h->d_ht);
+    h->ht_bits = 0;
     free_csr(h);
     free_prev(h);
     h->N = 0;
@@ -922,7 +1023,8 @@ int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const 
         free_csr(h);
         dfree(h->d_up); dfree(h->d_dn); dfree(h->d_up_b); dfree(h->d_inv); dfree(h->d_diag);
         dfree(h->d_ga); dfree(h->d_ga_start); dfree(h->d_gb); dfree(h->d_gb_start); dfree(h->d_order_b);
-        dfree(h->d_pos_b); dfree(h->d_pa_start); dfree(h->d_pa_list);
+        dfree(h->d_pos_b); dfree(h->d_pa_start); dfree(h->d_pa_list); dfree(h->d_ht);
+        h->ht_bits = 0;
         h->N = 0;
     } else {
         free_dets(h);
@@ -942,6 +1044,21 @@ int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const 
         RQ_CUDA(h, cudaMemcpyAsync(d_dg, diag, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
     }
     int rc = h->W == 1 ? build_groups<1>(h, d_aos, d_dg) : build_groups<2>(h, d_aos, d_dg);
+    if (rc == RISQGPU_OK && h->W == 1) {
+        // determinant table for the opposite-spin search: at least 2n slots
+        int bits = 10;
+        while (((int64_t)1 << bits) < 2 * (int64_t)n) bits++;
+        if (bits > 31) {
+            h->err = "determinant table exceeds 2^31 slots";
+            rc = RISQGPU_ERR_INVALID;
+        } else {
+            h->ht_bits = bits;
+            RQ_TRY(dalloc(h, h->d_ht, (size_t)1 << bits));
+            RQ_CUDA(h, cudaMemsetAsync(h->d_ht, 0xff, sizeof(int32_t) << bits, h->stream));
+            k_ht_insert<<<grid_for(h, (int64_t)n), 256, 0, h->stream>>>((int64_t)n, h->d_ga, h->d_dn, bits, h->d_ht);
+            RQ_TRY(check_launch(h, "determinant table"));
+        }
+    }
     RQ_TRY(sync(h, "set_dets"));
     dfree(d_aos);
     dfree(d_dg);

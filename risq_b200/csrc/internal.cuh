@@ -80,6 +80,10 @@ struct risqgpu {
     int32_t* d_pa_start = nullptr;  // G_a + 1
     int32_t* d_pa_list = nullptr;
     size_t n_pa = 0;
+    // open-addressing table (alpha group, beta string) -> internal index, one-word
+    // strings only (norb <= 64); 2^ht_bits slots of int32, -1 = empty
+    int32_t* d_ht = nullptr;
+    int ht_bits = 0;
 
     // sparse H: both triangles, rows in internal order, diagonal separate
     int precision = -1;   // value storage: FP64, FP32, MIXED or COLS

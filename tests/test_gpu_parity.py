@@ -313,3 +313,23 @@ def test_upper_triangle_sigma_on_large_alpha_groups():
         g.build(_capi.FP32_UPPER)
         g.sigma_device(perm_free.data_ptr(), y32.data_ptr(), 1)
         assert np.max(np.abs(y32.double().cpu().numpy() - ref32)) <= 1e-5 * np.max(np.abs(ref32))
+
+
+@pytest.mark.parametrize("prec", [_capi.FP64, _capi.FP64_UPPER])
+def test_connection_set_with_table_search(prec):
+    """Alpha partner groups larger than 256 determinants are searched through the
+    (alpha group, beta string) table instead of scanned (build_h.cu): on a set with
+    such groups (n12 6a6b eps 1e-3, 30,925 dets, groups up to 591) the stored set and
+    every element equal the oracle's sparse H bitwise."""
+    ints, e, dets, coeffs, diag, log = H.synthetic_hci(12, 6, 1e-3)
+    _, counts = np.unique(dets[:, 0], return_counts=True)
+    assert (counts > 256).sum() > 0
+    sp = O.Sparse().build(H.oracle_ham(ints, 0), dets, diag, 0)
+    orp, ocols, ovals, _ = sp.export()
+    with _gpu(ints) as g:
+        g.set_dets(dets, 0, diag)
+        g.build(prec)
+        rp, cols, vals, _ = g.export_upper()
+    np.testing.assert_array_equal(rp, orp)
+    np.testing.assert_array_equal(cols, ocols)
+    np.testing.assert_array_equal(vals, ovals)
