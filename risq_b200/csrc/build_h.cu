@@ -181,15 +181,24 @@ __device__ __forceinline__ uint64_t det_hash(uint32_t g, uint64_t beta) {
     return h;
 }
 
-// Insert every determinant (one-word strings) into the open-addressing table.
+// Insert every determinant (one-word strings) into the open-addressing table.  A slot
+// is {beta low, beta high, alpha group, internal index} (16 bytes, one vector load per
+// probe); index -1 marks an empty slot.
 __global__ void k_ht_insert(int64_t n, const int32_t* __restrict__ ga, const uint64_t* __restrict__ dn, int bits,
-                            int32_t* __restrict__ ht) {
+                            int4* __restrict__ ht) {
     const uint32_t mask = (1u << bits) - 1u;
     for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n; q += (int64_t)gridDim.x * blockDim.x) {
-        uint32_t slot = (uint32_t)(det_hash((uint32_t)ga[q], dn[q]) >> (64 - bits));
+        const uint64_t beta = dn[q];
+        const int g = ga[q];
+        uint32_t slot = (uint32_t)(det_hash((uint32_t)g, beta) >> (64 - bits));
         // the table has at least 2n slots, so an empty one is always found
         for (uint32_t t = 0; t <= mask; t++) {
-            if (atomicCAS(ht + slot, -1, (int32_t)q) == -1) break;
+            if (atomicCAS(&ht[slot].w, -1, (int32_t)q) == -1) {
+                ht[slot].x = (int)(uint32_t)beta;
+                ht[slot].y = (int)(uint32_t)(beta >> 32);
+                ht[slot].z = g;
+                break;
+            }
             slot = (slot + 1) & mask;
         }
     }
@@ -213,7 +222,7 @@ struct SetView {
     int64_t nsh;
     int norb;
     // (alpha group, beta string) -> internal index, or null (two-word strings)
-    const int32_t* __restrict__ ht;
+    const int4* __restrict__ ht;
     int ht_bits;
     // previous build (incremental extension)
     const int32_t* __restrict__ prev_inv_of_caller;  // caller -> previous internal (or null)
@@ -248,10 +257,11 @@ struct SetView {
     __device__ __forceinline__ int find(int g, uint64_t beta) const {
         const uint32_t mask = (1u << ht_bits) - 1u;
         uint32_t slot = (uint32_t)(det_hash((uint32_t)g, beta) >> (64 - ht_bits));
+        const int lo = (int)(uint32_t)beta, hi = (int)(uint32_t)(beta >> 32);
         for (uint32_t t = 0; t <= mask; t++) {
-            const int q = __ldg(ht + slot);
-            if (q < 0) return -1;
-            if (__ldg(ga + q) == g && __ldg(dn + q) == beta) return q;
+            const int4 e = __ldg(ht + slot);
+            if (e.w < 0) return -1;
+            if (e.x == lo && e.y == hi && e.z == g) return e.w;
             slot = (slot + 1) & mask;
         }
         return -1;
@@ -1054,7 +1064,7 @@ int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const 
         } else {
             h->ht_bits = bits;
             RQ_TRY(dalloc(h, h->d_ht, (size_t)1 << bits));
-            RQ_CUDA(h, cudaMemsetAsync(h->d_ht, 0xff, sizeof(int32_t) << bits, h->stream));
+            RQ_CUDA(h, cudaMemsetAsync(h->d_ht, 0xff, sizeof(int4) << bits, h->stream));
             k_ht_insert<<<grid_for(h, (int64_t)n), 256, 0, h->stream>>>((int64_t)n, h->d_ga, h->d_dn, bits, h->d_ht);
             RQ_TRY(check_launch(h, "determinant table"));
         }

@@ -81,8 +81,9 @@ struct risqgpu {
     int32_t* d_pa_list = nullptr;
     size_t n_pa = 0;
     // open-addressing table (alpha group, beta string) -> internal index, one-word
-    // strings only (norb <= 64); 2^ht_bits slots of int32, -1 = empty
-    int32_t* d_ht = nullptr;
+    // strings only (norb <= 64); 2^ht_bits slots {beta lo, beta hi, group, index},
+    // index -1 = empty
+    int4* d_ht = nullptr;
     int ht_bits = 0;
 
     // sparse H: both triangles, rows in internal order, diagonal separate
