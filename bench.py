@@ -111,6 +111,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(sm)}
 
 
+def max_over_ranks(x, world):
+    """The largest x over the ranks: a replicated step lasts as long as its slowest rank.
+    Every rank calls it at the same point (NCCL reduces on the GPU, gloo on the CPU)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def det_set(cfg_id, device, log=print):
     """The HCI determinant set of a config, made by this library's device variational stage."""
     from risq_b200 import GpuHam, _capi
@@ -276,10 +289,7 @@ def main():
     torch.cuda.synchronize()
     ms = t_start.elapsed_time(t_end) / args.steps
     clk = clocks.stop()
-    mx = torch.tensor([ms], device="cuda")
-    if world > 1:
-        dist.all_reduce(mx, op=dist.ReduceOp.MAX)
-    ms_max = float(mx.item())
+    ms_max = max_over_ranks(ms, world)
     barrier()
     hs_m, r_m = runs[-1]
     e_m = float(r_m.eigenvalues[0])
@@ -382,10 +392,7 @@ def main():
         torch.cuda.synchronize()
         e2e_ms.append(a.elapsed_time(b))
     e2e = float(np.mean(e2e_ms))
-    et = torch.tensor([e2e], device="cuda")
-    if world > 1:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-    e2e = float(et.item())
+    e2e = max_over_ranks(e2e, world)
 
     storage = {_capi.FP64: "FP64 both triangles", _capi.FP64_UPPER: "FP64 upper triangle",
                _capi.COLS: "columns only, FP64 elements recomputed in sigma",

@@ -112,3 +112,40 @@ def test_oracle_hci_log_shape():
     assert [l["ndets"] for l in log] == sorted(l["ndets"] for l in log)
     assert log[-1]["ndets"] == len(dets)
     assert abs(np.linalg.norm(coeffs) - 1.0) < 1e-10
+
+
+def _rank_main(rank, world, port, out):
+    import os
+
+    import torch.distributed as dist
+
+    import bench
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # each replica reports its own step time; every rank must see the slowest one
+        out[rank] = bench.max_over_ranks(10.0 + 5.0 * rank, world)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_replica_timing_takes_the_max_over_ranks():
+    """bench.py --gpus N runs one replica per rank and reports the slowest rank's time
+    (two gloo ranks on the CPU)."""
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    assert out[0] == 15.0 and out[1] == 15.0
+    import bench
+    assert bench.max_over_ranks(7.5, 1) == 7.5  # one GPU: no collective
