@@ -42,6 +42,10 @@ CONFIGS = {
     4: dict(n=32, nel=12, eps=1e-5),
 }
 DAV_MAX_ITER = 2000  # the reference's cap of 50 does not converge on these integrals
+# DRAM bytes per algorithmic byte of the upper-triangle FP32 sigma, from one ncu capture
+# (config 0 set, 5.82e7 stored pairs: 472.3 MB read + 4.1 MB written for 470 MB); the
+# stream grows with the stored pairs, so the ratio carries to larger sets
+UPPER_FP32_TRAFFIC_RATIO = 476.4 / 470.0
 
 
 def peaks():
@@ -423,7 +427,11 @@ def main():
         "roofline": {"bound": "hbm",
                      "kernel": "k_spmv<FP32>" if full_m else "k_spmv_upper<FP32>",
                      "achieved": sig32_gbs, "peak": peak, "unit": "GB/s",
-                     "frac": sig32_gbs / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": sig32_gbs / peak, "peak_kind": peak_kind,
+                     "traffic": None if full_m else int(b_sig32 * UPPER_FP32_TRAFFIC_RATIO),
+                     "traffic_source": None if full_m else
+                     "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_spmv_upper<float, float> on the "
+                     "config 0 set (476.4 MB for 470 MB algorithmic), scaled by the stored pairs",
                      "bytes_per_launch": int(b_sig32), "ms_per_launch": t_sig32},
         "time_to_evar_ms": {"mixed_learned": ms_max, "fp64_plain": ms_plain, "mixed_dpr": ms_mixed_dpr,
                             "mixed_dpr_iters": r_md.stats["iters"],
