@@ -18,7 +18,11 @@
 // per column); one sigma; one pass for the new projected column.  All
 // reductions are two-stage with a fixed grid, so results are reproducible.
 // The restart takes H*ritz as the combination of the stored H*V columns rather
-// than a fresh sigma (same vector, one sigma fewer).
+// than a fresh sigma (same vector, one sigma fewer).  The host waits twice per
+// iteration: for the residual norms (convergence test) and for the new projected
+// column, which arrives together with the squared norm of the new vector; the
+// reference's dependent-vector exit is therefore taken after that vector's sigma,
+// whose result is dropped.
 //
 // MIXED mode keeps V and H*V in FP32 and runs the FP32 sigma; dots, Gram-Schmidt
 // coefficients, the projected matrix and the Ritz vectors stay FP64.  After it
@@ -28,6 +32,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "internal.cuh"
@@ -39,22 +44,37 @@ int mlp_scale_impl(risqgpu* h, double energy, float* out);
 
 namespace {
 
-// sigma with CUDA-event timing accumulated into the handle
-int timed_sigma(risqgpu* h, const void* x, void* y, int kind) {
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    cudaEventRecord(a, h->stream);
-    int rc = sigma_device(h, x, y, kind);
-    cudaEventRecord(b, h->stream);
-    cudaEventSynchronize(b);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
-    h->sigma_ms_acc += ms;
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    return rc;
-}
+// sigma bracketed by CUDA events on the handle's stream; the events are read once the
+// solve has finished (no synchronisation per sigma)
+struct SigmaTimer {
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    int run(risqgpu* h, const void* x, void* y, int kind) {
+        cudaEvent_t a, b;
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+        cudaEventRecord(a, h->stream);
+        int rc = sigma_device(h, x, y, kind);
+        cudaEventRecord(b, h->stream);
+        ev.emplace_back(a, b);
+        return rc;
+    }
+    // after the stream has been synchronised
+    void collect(risqgpu* h) {
+        for (auto& e : ev) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, e.first, e.second) == cudaSuccess) h->sigma_ms_acc += ms;
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+        ev.clear();
+    }
+    ~SigmaTimer() {
+        for (auto& e : ev) {
+            cudaEventDestroy(e.first);
+            cudaEventDestroy(e.second);
+        }
+    }
+};
 
 constexpr int KMAX = 24;   // basis columns (nroots <= 8 -> at most 18)
 constexpr int RMAX = 8;    // roots
@@ -292,6 +312,12 @@ struct Work {
     double* red = nullptr;      // KMAX+1
     double* small = nullptr;    // Y + lambda
     double* coef = nullptr;     // KMAX+1
+    double* cols = nullptr;     // (RMAX + KMAX) x (KMAX+1): reduced projected columns, then saved norms
+    SigmaTimer timer;
+    int reduce_to(int m, double* dev_out) {
+        k_reduce<<<m, DBLK, 0, h->stream>>>(partial, grid, m, KMAX + 1, dev_out);
+        return check_launch(h, "reduce");
+    }
     int reduce(int m, double* host_out) {
         k_reduce<<<m, DBLK, 0, h->stream>>>(partial, grid, m, KMAX + 1, red);
         RQ_TRY(check_launch(h, "reduce"));
@@ -355,19 +381,33 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
             }
         }
     }
-    for (int c = 0; c < dim; c++) RQ_TRY(timed_sigma(h, V + (size_t)c * N, HV + (size_t)c * N, sigma_kind));
+    for (int c = 0; c < dim; c++) RQ_TRY(wk.timer.run(h, V + (size_t)c * N, HV + (size_t)c * N, sigma_kind));
     out.n_sigma += dim;
     std::vector<double> P((size_t)KMAX * KMAX, 0.0);
-    auto proj_cols = [&](int c0, int c1, int m) -> int {  // P[i][c] for i < m, c in [c0, c1)
-        std::vector<double> col(KMAX + 1);
+    // P[i][c] for i < m, c in [c0, c1): every column reduced on the device, then one copy
+    // to the host, which also brings the saved squared norm of the last new vector
+    // (slot `extra` of the buffer, when extra >= 0)
+    double saved_norm2 = 0.0;
+    auto proj_cols = [&](int c0, int c1, int m, int extra) -> int {
+        const int nc = c1 - c0;
         for (int c = c0; c < c1; c++) {
             k_multidot<T><<<g, DBLK, 0, h->stream>>>(V, m, HV + (size_t)c * N, N, wk.partial);
-            RQ_TRY(wk.reduce(m, col.data()));
-            for (int i = 0; i < m; i++) { P[i * KMAX + c] = col[i]; P[c * KMAX + i] = col[i]; }
+            RQ_TRY(wk.reduce_to(m, wk.cols + (size_t)(c - c0) * (KMAX + 1)));
         }
+        const int nread = extra >= 0 ? extra + 1 : nc * (KMAX + 1);
+        std::vector<double> buf((size_t)nread);
+        RQ_CUDA(h, cudaMemcpyAsync(buf.data(), wk.cols, sizeof(double) * nread, cudaMemcpyDeviceToHost, h->stream));
+        RQ_TRY(sync(h, "projected columns"));
+        for (int c = c0; c < c1; c++)
+            for (int i = 0; i < m; i++) {
+                const double v = buf[(size_t)(c - c0) * (KMAX + 1) + i];
+                P[i * KMAX + c] = v;
+                P[c * KMAX + i] = v;
+            }
+        if (extra >= 0) saved_norm2 = buf[extra];
         return RISQGPU_OK;
     };
-    RQ_TRY(proj_cols(0, dim, dim));
+    RQ_TRY(proj_cols(0, dim, dim, -1));
     std::vector<double> last(nr, 0.0);
     if (last_init) for (int c = 0; c < nr; c++) last[c] = last_init[c];
     std::vector<double> w(KMAX), Y(KMAX * KMAX), Pd(KMAX * KMAX), hostsmall(KMAX * RMAX + RMAX);
@@ -428,7 +468,8 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
         for (int c = 0; c < nr; c++) last[c] = w[c];
         if (room) {
             if (std::sqrt(red[nr]) < 1e-9) { out.converged = true; out.reason = 1; break; }
-            bool redundant = false;
+            // slot of the last new vector's squared norm: after the nr projected columns
+            const int norm_slot = nr * (KMAX + 1);
             for (int c = 0; c < nr; c++) {
                 const int col = dim + c;
                 T* t = V + (size_t)col * N;
@@ -439,18 +480,20 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
                 RQ_TRY(wk.reduce(col + 1, nullptr));
                 RQ_CUDA(h, cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * col, cudaMemcpyDeviceToDevice, h->stream));
                 k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, col, t, N, wk.coef, wk.partial);
-                double nrm2 = 0.0;
-                k_reduce<<<col + 1, DBLK, 0, h->stream>>>(wk.partial, g, col + 1, KMAX + 1, wk.red);
-                RQ_CUDA(h, cudaMemcpyAsync(&nrm2, wk.red + col, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-                RQ_TRY(sync(h, "cgs"));
-                if (c == nr - 1 && std::sqrt(nrm2) < 1e-9) { redundant = true; break; }
+                RQ_TRY(wk.reduce(col + 1, nullptr));
+                if (c == nr - 1)
+                    RQ_CUDA(h, cudaMemcpyAsync(wk.cols + norm_slot, wk.red + col, sizeof(double),
+                                               cudaMemcpyDeviceToDevice, h->stream));
                 k_scale<T><<<g, DBLK, 0, h->stream>>>(t, N, wk.red + col);
             }
-            if (redundant) { out.converged = true; out.reason = 2; break; }
             for (int c = 0; c < nr; c++)
-                RQ_TRY(timed_sigma(h, V + (size_t)(dim + c) * N, HV + (size_t)(dim + c) * N, sigma_kind));
+                RQ_TRY(wk.timer.run(h, V + (size_t)(dim + c) * N, HV + (size_t)(dim + c) * N, sigma_kind));
+            RQ_TRY(proj_cols(dim, dim + nr, dim + nr, norm_slot));
+            // a dependent last vector (MGS norm < 1e-9, modified_gram_schmidt.rs:22-36) ends the
+            // solve; its sigma and projected column, computed before the norm reached the host,
+            // are dropped, so the result is the one of stopping before them
+            if (std::sqrt(saved_norm2) < 1e-9) { out.converged = true; out.reason = 2; break; }
             out.n_sigma += nr;
-            RQ_TRY(proj_cols(dim, dim + nr, dim + nr));
             dim += nr;
         } else {
             // restart to the Ritz vectors
@@ -458,7 +501,7 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
             RQ_TRY(check_launch(h, "restart"));
             dim = nr;
             std::fill(P.begin(), P.end(), 0.0);
-            RQ_TRY(proj_cols(0, dim, dim));
+            RQ_TRY(proj_cols(0, dim, dim, -1));
         }
     }
     out.iters += it + (it < max_iter ? 1 : 0);
@@ -500,6 +543,7 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
     RQ_TRY(dalloc(h, wk.red, KMAX + 1));
     RQ_TRY(dalloc(h, wk.small, KMAX * RMAX + RMAX));
     RQ_TRY(dalloc(h, wk.coef, KMAX + 1));
+    RQ_TRY(dalloc(h, wk.cols, (size_t)(KMAX + 2) * (KMAX + 1)));
     double *ritz = nullptr, *hr = nullptr, *init_int = nullptr, *tmp = nullptr;
     RQ_TRY(dalloc(h, ritz, (size_t)nroots * N));
     RQ_TRY(dalloc(h, hr, (size_t)nroots * N));
@@ -552,7 +596,8 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         dfree(outv);
     }
     RQ_TRY(sync(h, "davidson end"));
-    dfree(wk.partial); dfree(wk.red); dfree(wk.small); dfree(wk.coef);
+    wk.timer.collect(h);
+    dfree(wk.partial); dfree(wk.red); dfree(wk.small); dfree(wk.coef); dfree(wk.cols);
     dfree(ritz); dfree(hr); dfree(init_int); dfree(tmp); dfree(fscale);
     if (st) {
         st->iters = lo.iters;
