@@ -11,20 +11,27 @@ sparse-H build with FP32 values + FP32 remainder, then Davidson with FP32 sigma
 and FP32 basis (FP64 dots, Gram-Schmidt and Rayleigh-Ritz), the learned
 preconditioner (DPR fallback), and closing FP64-sigma sweeps, from the
 reference's default start until |r| < 1e-4 and |dE| < 1e-8.  The plain FP64
-path (FP64 build + the reference's DPR Davidson) is timed beside it on the same
-set, and the energy difference of the two is reported (it must stay <= 1 uHa).
+path (FP64 build + the reference's DPR Davidson with its 11-vector search
+space) is timed beside it on the same set, and the energy difference of the two
+is reported (it must stay <= 1 uHa).
 
 Metric: determinants solved per second = N_dets * steps / time (max over ranks),
 whole job.  With N GPUs every rank solves its own replica (the single-GPU path
-does not shard), so scaling is weak.  Extra keys: both solve times and their
-ratio, sigma GB/s against the measured HBM peak, H-build elements/s.
+does not shard), so scaling is weak.  Extra keys: the solve times of every leg
+and their ratios, sigma GB/s against the measured HBM peak, H-build elements/s,
+and a same-set record: the GPU legs and the CPU oracle on the variational space
+of an earlier HCI iteration, which the CPU solves in seconds.
+
+--impl reference times the reference's algorithm on the host cores: the CPU
+oracle (a C restatement of the reference's Rust path, multi-threaded) runs its
+own HCI to that earlier iteration and each step solves that space, so the arm
+never loads the GPU library.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
-import subprocess
 import sys
 import threading
 import time
@@ -42,10 +49,13 @@ CONFIGS = {
     4: dict(n=32, nel=12, eps=1e-5),
 }
 DAV_MAX_ITER = 2000  # the reference's cap of 50 does not converge on these integrals
-# DRAM bytes per algorithmic byte of the upper-triangle FP32 sigma, from one ncu capture
-# (config 0 set, 5.82e7 stored pairs: 472.3 MB read + 4.1 MB written for 470 MB); the
-# stream grows with the stored pairs, so the ratio carries to larger sets
-UPPER_FP32_TRAFFIC_RATIO = 476.4 / 470.0
+# The CPU legs time the variational space of the last HCI iteration whose set holds at
+# most this many determinants (the whole set when it is smaller).
+CPU_SAMPLE_MAX = 150_000
+# Davidson search space of the product path (max_space, keep): a thick restart keeping
+# the lowest `keep` Ritz vectors; (0, 0) would be the reference's nroots + 10 with a
+# restart to the Ritz vector.  The FP32 basis vectors take half the memory of FP64 ones.
+PRODUCT_SPACE = (32, 8)
 
 
 def peaks():
@@ -55,6 +65,14 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def workload_config(cfg_id, world):
+    """The `config` dict both arms print (the workload, not how one arm stores it)."""
+    c = CONFIGS[cfg_id]
+    return {"workload": f"hci n{c['n']} {c['nel']}a{c['nel']}b eps_var {c['eps']:g} seed 0",
+            "step": "sparse-H build + Davidson to E_var (tol 1e-4, etol 1e-8) from the reference's default start",
+            "l2": "CSR stream larger than L2 every step", "parallelism": f"replicas x{world}"}
 
 
 class ClockSampler:
@@ -130,7 +148,7 @@ def max_over_ranks(x, world):
 
 def det_set(cfg_id, device, log=print):
     """The HCI determinant set of a config, made by this library's device variational stage."""
-    from risq_b200 import GpuHam, _capi
+    from risq_b200 import GpuHam
     from risq_b200.fcidump import synthetic_integrals
     c = CONFIGS[cfg_id]
     ints = synthetic_integrals(c["n"], 0)
@@ -141,7 +159,7 @@ def det_set(cfg_id, device, log=print):
         return ints, z["dets"], z["diag"], float(z["energy"]), list(z["log"])
     t0 = time.time()
     with GpuHam(ints, device) as g:
-        # precision -1: FP64 while the matrix fits, FP32 selection solves beyond that
+        # precision -1: FP64 while the matrix fits, then the upper triangle, then columns only
         e, dets, coeffs, diag, vlog = g.variational(c["nel"], c["nel"], c["eps"], max_iter=20,
                                                     dav_max_iter=DAV_MAX_ITER, precision=-1)
     log(f"# det set config {cfg_id}: N={len(dets)} E={e:.10f} ({time.time() - t0:.1f} s)")
@@ -153,53 +171,74 @@ def det_set(cfg_id, device, log=print):
     return ints, dets, diag, e, vlog
 
 
-def cpu_sample(ints, dets, diag, vlog, budget_s=20.0):
-    """Oracle (single-threaded C restatement) time-to-E_var on a prefix of the set.
+def sample_iteration(sizes):
+    """1-based HCI iteration (and its set size) that the CPU legs time: the last one whose
+    set holds at most CPU_SAMPLE_MAX determinants, or the final one."""
+    k, n = len(sizes), sizes[-1]
+    for i, s in enumerate(sizes):
+        if s <= CPU_SAMPLE_MAX:
+            k, n = i + 1, s
+    return k, n
 
-    The HCI list is ordered by selection, so a prefix whose length is one of the
-    earlier iterations' sizes is that iteration's variational space; the largest
-    such prefix the CPU solves within the budget is used."""
+
+def oracle_solve(oh, dets, diag):
+    """The reference algorithm on every host core: the oracle's fast-rule build and DPR
+    Davidson (search space 11, restart to the Ritz vector) from the reference's default
+    start.  Returns the time and the result."""
     from oracle import oracle as O
-    oh = O.Ham.from_arrays(ints.norb, 0, ints.nuc, ints.one_body, ints.two_body)
-    sizes = sorted({int(r["n_dets"]) for r in vlog if int(r["n_dets"]) > 2})
-    best = None
-    for n in sizes:
-        t0 = time.perf_counter()
-        sp = O.Sparse().build(oh, dets[:n], diag[:n], 0)
-        rc, ev, _, st = sp.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
-        t = time.perf_counter() - t0
-        best = dict(n=n, t=t, nnz=sp.nnz, iters=st["iters"], energy=float(ev[0]))
-        if t > budget_s / 4:
-            break
-    return best
+    t0 = time.perf_counter()
+    sp = O.Sparse().build_par(oh, dets, diag)
+    rc, ev, _, st = sp.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, parallel=True)
+    t = time.perf_counter() - t0
+    return dict(t=t, energy=float(ev[0]), iters=st["iters"], nnz=sp.nnz, converged=rc == 0)
 
 
 def run_reference(args):
-    """--impl reference: the CPU path of the reference algorithm on the host cores."""
+    """--impl reference: the reference's algorithm (the CPU oracle, every host core) makes its
+    own HCI space and times solves of it; the GPU library is never loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    from oracle import oracle as O
+    from risq_b200.fcidump import synthetic_integrals
     cfg = CONFIGS[args.config]
-    ints, dets, diag, e_gpu, vlog = det_set(args.config, 0, log=lambda *a: None)
-    times = []
-    sample = None
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    ints = synthetic_integrals(cfg["n"], 0)
+    oh = O.Ham.from_arrays(ints.norb, 0, ints.nuc, ints.one_body, ints.two_body)
+    # the reference's HCI loop (variational, src/var/mod.rs:59-134) on the host cores, up to the
+    # last iteration whose space holds at most CPU_SAMPLE_MAX determinants
+    t0 = time.perf_counter()
+    hci = O.Hci(oh, cfg["nel"], cfg["nel"], cfg["eps"]).set_options(DAV_MAX_ITER, parallel=True)
+    prev = None
+    for it in range(20):
+        if hci.step():
+            break
+        if hci.ndets > CPU_SAMPLE_MAX:
+            break
+        prev = (it + 1, hci.export())
+    if prev is None:  # the first iteration is already larger than the sample bound
+        prev = (1, hci.export())
+    t_hci = time.perf_counter() - t0
+    k, (dets, coeffs, diag) = prev
+    n = len(dets)
+    times, s = [], None
     for i in range(args.warmup + args.steps):
-        s = cpu_sample(ints, dets, diag, vlog)
+        s = oracle_solve(oh, dets, diag)
         if i >= args.warmup:
             times.append(s["t"])
-            sample = s
     t = float(np.mean(times))
-    v = sample["n"] / t
+    v = n / t
+    threads = O.num_threads()
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "dets/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"hci n{cfg['n']} {cfg['nel']}a{cfg['nel']}b eps_var {cfg['eps']:g} seed 0",
-                   "sample_prefix_dets": sample["n"], "full_dets": int(len(dets))},
-        "cpu_baseline": {"value": v, "unit": "dets/s", "cores": 1, "kind": "port",
-                         "sample": f"H build + DPR Davidson on the first {sample['n']} of {len(dets)} determinants "
-                                   f"(an earlier HCI iteration's space; {sample['nnz']} upper elements, "
-                                   f"{sample['iters']} Davidson iterations)"},
+        "config": workload_config(args.config, world),
+        "cpu_baseline": {"value": v, "unit": "dets/s", "cores": threads, "kind": "port",
+                         "sample": f"the variational space of HCI iteration {k} ({n} determinants, {s['nnz']} "
+                                   f"upper elements), made by the oracle's own HCI ({t_hci:.0f} s, untimed); "
+                                   f"each step builds H and runs DPR Davidson to E_var ({s['iters']} iterations, "
+                                   f"E = {s['energy']:.10f})"},
         "e2e": {"value": v, "unit": "dets/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -212,10 +251,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--impl", default="risq_b200")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle legs")
     ap.add_argument("--storage", choices=["auto", "upper"], default="auto",
                     help="auto: both triangles when they fit, else the upper triangle; upper: always the "
-                         "upper triangle (the reference's SparseMatUpperTri layout)")
+                         "upper triangle (the reference's SparseMatUpperTri layout, tiled for sigma)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -229,7 +268,7 @@ def main():
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    from risq_b200 import GpuHam, _capi
+    from risq_b200 import GpuHam, _capi, learned
 
     def barrier():
         if world > 1:
@@ -251,7 +290,6 @@ def main():
     g = GpuHam(ints, local)
     g.set_stream(stream.cuda_stream)
     ev = lambda: torch.cuda.Event(enable_timing=True)
-    from risq_b200 import learned
     model = learned.load_default(ints.norb)
     if model is not None:
         learned.install(g, model)
@@ -269,15 +307,29 @@ def main():
                 say(f"# storage {pr} does not fit one GPU")
         raise RuntimeError("no storage mode fits")
 
+    def timed(fn):
+        a, b = ev(), ev()
+        torch.cuda.synchronize()
+        a.record(stream)
+        out = fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b), out
+
     # product path storage: FP32 + FP32 remainder rows when both triangles fit, else the
-    # upper triangle (the reference's SparseMatUpperTri layout)
+    # upper triangle (the reference's SparseMatUpperTri layout, regrouped into tiles)
     upper_only = args.storage == "upper"
     precm = first_fitting([_capi.MIXED_UPPER] if upper_only else [_capi.MIXED, _capi.MIXED_UPPER])
 
-    def product_step():
-        hs = g.build(precm)
-        r = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=_capi.MODE_MIXED, precond=precond)
+    def solve(prec, mode, pc, space):
+        g.set_subspace(*space)
+        hs = g.build(prec)
+        r = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=mode, precond=pc)
+        g.set_subspace(0, 0)
         return hs, r
+
+    def product_step():
+        return solve(precm, _capi.MODE_MIXED, precond, PRODUCT_SPACE)
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -310,33 +362,26 @@ def main():
     except Exception as e:  # profiler unavailable: leave the count out rather than guess
         say(f"# launch count unavailable: {e}")
 
-    # ---- mixed precision with the plain DPR preconditioner (one untimed-loop run) ----
-    a, b = ev(), ev()
-    torch.cuda.synchronize()
-    a.record(stream)
-    g.build(precm)
-    r_md = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=_capi.MODE_MIXED)
-    b.record(stream)
-    torch.cuda.synchronize()
-    ms_mixed_dpr = a.elapsed_time(b)
+    # ---- other legs on the same set (one run each) ----
+    legs = {}
+    ms_l, (_, r_l) = timed(lambda: solve(precm, _capi.MODE_MIXED, _capi.PRECOND_DPR, PRODUCT_SPACE))
+    legs["mixed_dpr"] = (ms_l, r_l)
+    ms_l, (_, r_l) = timed(lambda: solve(precm, _capi.MODE_MIXED, precond, (0, 0)))
+    legs["mixed_learned_reference_space"] = (ms_l, r_l)
 
-    # ---- plain FP64 GPU path on the same set: FP64 build + the reference's DPR Davidson ----
+    # ---- plain FP64 GPU path: FP64 build + the reference's DPR Davidson (11-vector space) ----
     prec64 = first_fitting([_capi.FP64_UPPER, _capi.COLS] if upper_only else [_capi.FP64, _capi.FP64_UPPER, _capi.COLS])
     plain_ms, plain = [], None
     for i in range(2):
-        a, b = ev(), ev()
-        torch.cuda.synchronize()
-        a.record(stream)
-        hs64 = g.build(prec64)
-        r64 = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER)
-        b.record(stream)
-        torch.cuda.synchronize()
+        ms_p, out = timed(lambda: solve(prec64, _capi.MODE_FP64, _capi.PRECOND_DPR, (0, 0)))
         if i > 0:  # the first is a warm-up
-            plain_ms.append(a.elapsed_time(b))
-        plain = (hs64, r64)
+            plain_ms.append(ms_p)
+        plain = out
     hs64, r64 = plain
     e64 = float(r64.eigenvalues[0])
     ms_plain = float(np.mean(plain_ms))
+    ms_l, (_, r_l) = timed(lambda: solve(prec64, _capi.MODE_FP64, _capi.PRECOND_DPR, PRODUCT_SPACE))
+    legs["fp64_product_space"] = (ms_l, r_l)
 
     # ---- sigma roofline, FP64 (x, y in the library's internal order) ----
     nnz_u, nnz_f = g.nnz()
@@ -347,35 +392,34 @@ def main():
     def time_sigma(xx, yy, kind):
         for _ in range(3):
             g.sigma_device(xx.data_ptr(), yy.data_ptr(), kind)
-        a, b = ev(), ev()
-        torch.cuda.synchronize()
-        a.record(stream)
-        for _ in range(R):
-            g.sigma_device(xx.data_ptr(), yy.data_ptr(), kind)
-        b.record(stream)
-        torch.cuda.synchronize()
-        return a.elapsed_time(b) / R
+        ms_s, _ = timed(lambda: [g.sigma_device(xx.data_ptr(), yy.data_ptr(), kind) for _ in range(R)])
+        return ms_s / R
 
     t_sig = time_sigma(x, y, 0)
-    # algorithmic bytes: values (none when recomputed) + int32 columns, per row int64
-    # start + int32 length, x and diag read once, y written once; the recomputing
-    # kernel also reads both strings of every determinant once (N * 16 B)
-    if prec64 == _capi.FP64:
-        b_sig = nnz_f * (8 + 4) + N * (8 + 4) + 3 * N * 8
-    elif prec64 == _capi.FP64_UPPER:  # each pair once; y is read-modify-written in L2
-        b_sig = nnz_u * (8 + 4) + N * (8 + 4) + 3 * N * 8
-    else:
-        b_sig = nnz_f * 4 + N * (8 + 4) + 3 * N * 8 + N * 16
+    tiles64 = int(hs64.get("n_tiles", 0))
+
+    # algorithmic bytes of one sigma: values + int32 column / element index of every stored
+    # element, per row its start and length (12 B), x and the diagonal read once, y written
+    # once; tiled upper storage also reads 16 B per tile header; the recomputing kernel
+    # reads both strings of every determinant once (N * 16 B)
+    def sigma_bytes(prec, s_v, s_x, n_tiles):
+        if prec in (_capi.FP64, _capi.MIXED, _capi.FP32):
+            return nnz_f * (s_v + 4) + N * 12 + N * (2 * s_x + 8)
+        if prec in (_capi.FP64_UPPER, _capi.MIXED_UPPER, _capi.FP32_UPPER):
+            return nnz_u * (s_v + 4) + N * 12 + N * (2 * s_x + 8) + 16 * n_tiles
+        return nnz_f * 4 + N * 12 + N * (2 * s_x + 8) + N * 16
+
+    b_sig = sigma_bytes(prec64, 8, 8, tiles64)
     peak, peak_kind = peaks()
     sig_gbs = b_sig / (t_sig * 1e-3) / 1e9
 
     # ---- sigma roofline, FP32 (the product path's dominant kernel) ----
-    g.build(precm)
+    hs_p = g.build(precm)
     x32 = x.float()
     y32 = torch.empty_like(x32)
     t_sig32 = time_sigma(x32, y32, 1)
     full_m = precm == _capi.MIXED
-    b_sig32 = (nnz_f if full_m else nnz_u) * (4 + 4) + N * (8 + 4) + N * (4 + 4 + 8)
+    b_sig32 = sigma_bytes(precm, 4, 4, int(hs_p.get("n_tiles", 0)))
     sig32_gbs = b_sig32 / (t_sig32 * 1e-3) / 1e9
 
     # ---- end to end through the public API: host dets in, energy + coefficients out ----
@@ -385,23 +429,48 @@ def main():
     pin_diag.numpy()[:] = diag
     dets_pinned = pin.numpy().view(np.uint64)
     e2e_ms = []
+    g.set_subspace(*PRODUCT_SPACE)
     for i in range(max(1, min(args.steps, 2))):
-        torch.cuda.synchronize()
-        a, b = ev(), ev()
-        a.record(stream)
-        g.set_dets(dets_pinned, 0, pin_diag.numpy())
-        e_api, c_api, _, _ = g.sparse_optimize(None, 1e-4, 1e-8, max_iter=DAV_MAX_ITER, precision=precm,
-                                               mode=_capi.MODE_MIXED, precond=precond)
-        b.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms.append(a.elapsed_time(b))
-    e2e = float(np.mean(e2e_ms))
-    e2e = max_over_ranks(e2e, world)
+        def api_call():
+            g.set_dets(dets_pinned, 0, pin_diag.numpy())
+            return g.sparse_optimize(None, 1e-4, 1e-8, max_iter=DAV_MAX_ITER, precision=precm,
+                                     mode=_capi.MODE_MIXED, precond=precond)
+        ms_e, _ = timed(api_call)
+        e2e_ms.append(ms_e)
+    g.set_subspace(0, 0)
+    e2e = max_over_ranks(float(np.mean(e2e_ms)), world)
 
-    storage = {_capi.FP64: "FP64 both triangles", _capi.FP64_UPPER: "FP64 upper triangle",
+    # ---- same set as the CPU sample: an earlier HCI iteration's variational space ----
+    sizes = [int(r["n_dets"]) for r in vlog]
+    k_s, n_s = sample_iteration(sizes)
+    same = None
+    cpu = None
+    if rank == 0:
+        sd, sg = dets[:n_s], diag[:n_s]
+        g.set_dets(sd, 0, sg)
+        pm_s = _capi.MIXED if not upper_only else _capi.MIXED_UPPER
+        p64_s = _capi.FP64 if not upper_only else _capi.FP64_UPPER
+        for _ in range(2):  # warm-up, then timed
+            ms_sp, (_, r_sp) = timed(lambda: solve(pm_s, _capi.MODE_MIXED, precond, PRODUCT_SPACE))
+            ms_s64, (hs_s64, r_s64) = timed(lambda: solve(p64_s, _capi.MODE_FP64, _capi.PRECOND_DPR, (0, 0)))
+        same = {"hci_iteration": k_s, "n_dets": n_s, "nnz_upper": int(hs_s64["nnz_upper"]),
+                "gpu_product_ms": ms_sp, "gpu_product_iters": r_sp.stats["iters"],
+                "gpu_fp64_plain_ms": ms_s64, "gpu_fp64_iters": r_s64.stats["iters"],
+                "e_gpu_fp64": float(r_s64.eigenvalues[0]), "e_gpu_product": float(r_sp.eigenvalues[0])}
+        if not args.no_cpu:
+            from oracle import oracle as O
+            oh = O.Ham.from_arrays(ints.norb, 0, ints.nuc, ints.one_body, ints.two_body)
+            cpu = oracle_solve(oh, sd, sg)
+            same.update({"cpu_oracle_ms": 1000 * cpu["t"], "cpu_oracle_iters": cpu["iters"],
+                         "cpu_threads": O.num_threads(), "e_cpu_oracle": cpu["energy"],
+                         "dE_gpu_fp64_vs_oracle_uHa": abs(float(r_s64.eigenvalues[0]) - cpu["energy"]) * 1e6,
+                         "nnz_oracle": int(cpu["nnz"]),
+                         "ratio_cpu_vs_gpu_product": 1000 * cpu["t"] / ms_sp})
+
+    storage = {_capi.FP64: "FP64 both triangles", _capi.FP64_UPPER: "FP64 upper triangle, tiled",
                _capi.COLS: "columns only, FP64 elements recomputed in sigma",
                _capi.MIXED: "FP32 + FP32 remainder, both triangles",
-               _capi.MIXED_UPPER: "FP32 + FP32 remainder, upper triangle"}
+               _capi.MIXED_UPPER: "FP32 + FP32 remainder, upper triangle, tiled"}
     line = {
         "metric": METRIC,
         "value": N * world / (ms_max * 1e-3),
@@ -415,53 +484,58 @@ def main():
         "vs_baseline": None,
         "dtype": "f32 sigma / f64 dots, Rayleigh-Ritz and closing sweeps",
         "data": "synthetic",
-        "config": {"workload": f"hci n{cfg['n']} {cfg['nel']}a{cfg['nel']}b eps_var {cfg['eps']:g} seed 0",
-                   "n_dets": int(N), "nnz_upper": int(nnz_u), "nnz_full": int(nnz_f),
-                   "step": "mixed-precision sparse-H build + Davidson (FP32 sigma, learned preconditioner, "
-                           "closing FP64 sweeps) to E_var (tol 1e-4, etol 1e-8)",
-                   "precond": "learned (MLP, DPR fallback)" if model is not None else "DPR (no network for norb)",
-                   "storage": storage[precm], "fp64_storage": storage[prec64],
-                   "l2": "CSR stream larger than L2 every step", "parallelism": f"replicas x{world}"},
+        "config": workload_config(args.config, world),
+        "set": {"n_dets": int(N), "nnz_upper": int(nnz_u), "nnz_full": int(nnz_f),
+                "storage": storage[precm], "fp64_storage": storage[prec64],
+                "precond": "learned (MLP, DPR fallback)" if model is not None else "DPR (no network for norb)",
+                "product_space": {"max_space": PRODUCT_SPACE[0], "keep": PRODUCT_SPACE[1]}},
         "e2e": {"value": N * world / (e2e * 1e-3), "unit": "dets/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": int(N * 40), "d2h_bytes_per_step": int(N * 8 + 8)},
         "roofline": {"bound": "hbm",
-                     "kernel": "k_spmv<FP32>" if full_m else "k_spmv_upper<FP32>",
+                     "kernel": "k_spmv<FP32>" if full_m else "k_sigma_tiles<FP32>",
                      "achieved": sig32_gbs, "peak": peak, "unit": "GB/s",
                      "frac": sig32_gbs / peak, "peak_kind": peak_kind,
-                     "traffic": None if full_m else int(b_sig32 * UPPER_FP32_TRAFFIC_RATIO),
-                     "traffic_source": None if full_m else
-                     "ncu dram__bytes_read.sum + dram__bytes_write.sum of k_spmv_upper<float, float> on the "
-                     "config 0 set (476.4 MB for 470 MB algorithmic), scaled by the stored pairs",
+                     "traffic": None,
                      "bytes_per_launch": int(b_sig32), "ms_per_launch": t_sig32},
-        "time_to_evar_ms": {"mixed_learned": ms_max, "fp64_plain": ms_plain, "mixed_dpr": ms_mixed_dpr,
-                            "mixed_dpr_iters": r_md.stats["iters"],
-                            "dE_mixed_dpr_vs_fp64_uHa": abs(float(r_md.eigenvalues[0]) - e64) * 1e6,
+        "time_to_evar_ms": {"mixed_learned": ms_max, "fp64_plain": ms_plain,
                             "speedup_vs_fp64_plain": ms_plain / ms_max,
                             "dE_vs_fp64_uHa": abs(e_m - e64) * 1e6,
                             "mixed_iters": r_m.stats["iters"], "fp64_iters": r64.stats["iters"],
                             "mixed_fp64_sigmas": r_m.stats["n_sigma_fp64"],
                             "learned_fallbacks": r_m.stats["learned_fallbacks"],
-                            "mixed_build_ms": hs_m["ms_total"], "fp64_build_ms": hs64["ms_total"]},
-        "sigma": {"fp64_kernel": {_capi.FP64: "k_spmv<FP64>", _capi.FP64_UPPER: "k_spmv_upper<FP64>",
+                            "mixed_build_ms": hs_m["ms_total"], "fp64_build_ms": hs64["ms_total"],
+                            "legs": {k: {"ms": v[0], "iters": v[1].stats["iters"],
+                                         "dE_vs_fp64_uHa": abs(float(v[1].eigenvalues[0]) - e64) * 1e6}
+                                     for k, v in legs.items()}},
+        "sigma": {"fp64_kernel": {_capi.FP64: "k_spmv<FP64>", _capi.FP64_UPPER: "k_sigma_tiles<FP64>",
                                   _capi.COLS: "k_spmv_otf"}[prec64],
                   "fp64_gbs": sig_gbs, "fp64_ms": t_sig, "fp64_frac": sig_gbs / peak,
-                  "fp32_gbs": sig32_gbs, "fp32_ms": t_sig32, "fp32_frac": sig32_gbs / peak},
+                  "fp32_gbs": sig32_gbs, "fp32_ms": t_sig32, "fp32_frac": sig32_gbs / peak,
+                  "tiles": int(hs_p.get("n_tiles", 0)), "pairs_in_dense_tiles": int(hs_p.get("nnz_dense", 0))},
         "h_build": {"elems_per_s": (nnz_u + N) / (hs64["ms_total"] * 1e-3), "ms": hs64["ms_total"],
                     "gpu_ms_count": hs64["gpu_ms_count"], "gpu_ms_fill": hs64["gpu_ms_fill"],
                     "candidates": hs64["candidates"]},
         "davidson": {"energy_mixed": e_m, "energy_fp64": e64, "e_selection": e_sel,
                      "mixed_ms": r_m.stats["ms_total"], "mixed_ms_sigma": r_m.stats["ms_sigma"],
                      "fp64_ms": r64.stats["ms_total"], "fp64_ms_sigma": r64.stats["ms_sigma"]},
+        "same_set": same,
         "clocks": clk,
         "gpu_launches": launches_per_step * args.steps if launches_per_step is not None else None,
         "gpu_launches_per_step": launches_per_step,
     }
-    if rank == 0 and not args.no_cpu:
-        s = cpu_sample(ints, dets, diag, vlog)
-        line["cpu_baseline"] = {"value": s["n"] / s["t"], "unit": "dets/s", "cores": 1, "kind": "port",
-                                "sample": f"oracle H build + DPR Davidson on the first {s['n']} of {N} "
-                                          f"determinants ({s['nnz']} upper elements, {s['iters']} iterations, "
-                                          f"{s['t']:.1f} s)"}
+    if rank == 0 and cpu is not None:
+        # projection of the CPU time to the whole set: the oracle's time per stored pair and
+        # Davidson iteration on the sample, times the pairs and iterations of the full solve
+        per = cpu["t"] / (max(cpu["nnz"], 1) * max(cpu["iters"], 1))
+        proj_s = per * nnz_u * r64.stats["iters"]
+        line["cpu_baseline"] = {"value": n_s / cpu["t"], "unit": "dets/s", "cores": same["cpu_threads"],
+                                "kind": "port",
+                                "sample": f"oracle H build + DPR Davidson on the first {n_s} of {N} determinants "
+                                          f"(HCI iteration {k_s}; {cpu['nnz']} upper elements, {cpu['iters']} "
+                                          f"iterations, {cpu['t']:.1f} s)",
+                                "projected_full_set_s": proj_s,
+                                "projection": "sample seconds / (sample pairs x sample iterations) x full-set "
+                                              "pairs x plain-FP64 GPU iterations on the full set"}
     g.close()
     if rank == 0:
         print(json.dumps(line))

@@ -67,8 +67,10 @@ enum risqgpu_precision {
     RISQGPU_COLS = 3,   /* int32 columns only: the FP64 sigma recomputes every element on the fly
                            (bitwise the stored FP64 values) for sets whose values do not fit */
     /* Upper triangle only (each pair once, as the reference's SparseMatUpperTri): half the
-     * storage; sigma adds the transposed half with atomic adds into y (sums in a
-     * run-dependent order).  Built from scratch every time (no n_stored_h reuse). */
+     * storage.  The pairs are regrouped into row-panel x column-window tiles whose x and
+     * y windows sigma stages in shared memory; sums are formed in 64-bit fixed point, so
+     * sigma and the solves built on it are bitwise reproducible.  Built from scratch
+     * every time (no n_stored_h reuse). */
     RISQGPU_FP64_UPPER = 4,
     RISQGPU_FP32_UPPER = 5,
     RISQGPU_MIXED_UPPER = 6
@@ -106,7 +108,9 @@ typedef struct {
     double ms_total;
     uint64_t bytes_csr;       /* bytes written for columns + values */
     double gpu_ms_count;      /* CUDA-event durations on the handle's stream */
-    double gpu_ms_fill;
+    double gpu_ms_fill;       /* fill (and, for upper-triangle storage, the regrouping into tiles) */
+    uint64_t n_tiles;         /* upper-triangle storage: dense (row panel, column window) tiles */
+    uint64_t nnz_dense;       /* upper-triangle storage: stored pairs that lie in dense tiles */
 } risqgpu_hstats;
 
 typedef struct {
@@ -168,6 +172,16 @@ RISQGPU_API int risqgpu_nnz(const risqgpu_t* h, uint64_t* nnz_upper, uint64_t* n
  * FP32 modes export their stored values widened), diag[N] (nullable). */
 RISQGPU_API int risqgpu_export_upper(risqgpu_t* h, int64_t* rowptr, int64_t* cols, double* vals, size_t cap, double* diag);
 
+/* Export the stored elements of the given rows (caller indices, distinct) in both
+ * triangles: (out_row[i], out_col[i], out_val[i]) for every stored H_rc with r one of
+ * the rows, FP64 values (the FP32 modes widened, FP32 + remainder summed), in no
+ * particular order; *count receives the number of entries, and RISQGPU_ERR_CAPACITY
+ * is returned when it exceeds cap.  A row of the reference's SparseMatUpperTri
+ * (src/var/sparse.rs:24-36) together with the column of the same index: used to
+ * check sampled rows of sets too large to export whole.  Needs stored values. */
+RISQGPU_API int risqgpu_export_rows(risqgpu_t* h, const int64_t* rows, size_t k, int64_t* out_row, int64_t* out_col,
+                                    double* out_val, size_t cap, size_t* count);
+
 /* y = H x for nvec column vectors (FP64 host buffers, caller order). */
 RISQGPU_API int risqgpu_sigma(risqgpu_t* h, const double* x, double* y, int nvec);
 
@@ -192,6 +206,25 @@ RISQGPU_API int risqgpu_davidson(risqgpu_t* h, int nroots, const double* init, i
 RISQGPU_API int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coeff_eps, double energy_eps,
                             int max_iter, int precision, int mode, int precond, double* energy, double* coeffs,
                             risqgpu_hstats* hstats, risqgpu_dstats* dstats);
+
+/* Davidson search space of this handle's solves (risqgpu_davidson, sparse_optimize,
+ * variational).  max_space: basis vectors before a restart; keep: Ritz vectors kept
+ * at a restart.  0, 0 (the default) is the reference's Config::new, nroots + 10 and a
+ * restart to the nroots Ritz vectors (src/var/eigenvalues/algorithms/davidson.rs:53-79,
+ * :261-269).  A larger space with keep > nroots is a thick restart: the lowest `keep`
+ * Ritz vectors carry over, which keeps more of the Krylov information between
+ * restarts.  No counterpart in the reference beyond its fixed choice.  max_space <= 56,
+ * keep <= max_space / 2. */
+RISQGPU_API int risqgpu_set_subspace(risqgpu_t* h, int max_space, int keep);
+
+/* Bound the device memory this handle may hold (bytes; 0 = no bound beyond the
+ * device).  An allocation past the bound fails with RISQGPU_ERR_OOM, as a failed
+ * cudaMalloc would, and leaves the handle usable.  No counterpart in the reference:
+ * it lets a caller share one GPU between the library and its own work, and lets
+ * tests drive the out-of-memory paths without exhausting a shared device. */
+RISQGPU_API int risqgpu_set_memory_limit(risqgpu_t* h, size_t bytes);
+/* Device memory the handle holds now (used) and its bound (limit, 0 = none). */
+RISQGPU_API int risqgpu_memory_used(const risqgpu_t* h, size_t* used, size_t* limit);
 
 /* Run the handle's work on `stream` (a cudaStream_t on the handle's device; NULL
  * restores the handle's own stream), so that a caller can order and time it with
@@ -228,14 +261,19 @@ RISQGPU_API int risqgpu_var_log(risqgpu_t* h, risqgpu_var_iter* out, int cap, in
  * streams, where the cudaMalloc/cudaFree pair inside risqgpu_sigma would add a
  * device-wide synchronisation to every iteration.  x_dev and y_dev are device
  * pointers to N doubles in the caller's determinant order (allocated by the
- * caller); the two internal-order copies live in one static device array of 2 x
- * 2^20 doubles (16 MiB), held by every GPU that loads the library until the
- * process exits, so sets of more than 1,048,576 determinants are rejected with
- * RISQGPU_ERR_CAPACITY.  The first call on a device looks up that array's device
- * address (cudaGetSymbolAddress, with the handle's device current); make that
- * first call before any stream capture.  All calls share the array, so calls that
- * overlap on the GPU (other handles or threads, other streams) race; the contents
- * left by a previous call are never read.  Synchronous at return, like the others. */
+ * caller; x_dev may equal y_dev); the two internal-order copies live in one static
+ * device array of 2 x 2^20 doubles (16 MiB), held by every GPU that loads the
+ * library until the process exits, so sets of more than 1,048,576 determinants
+ * are rejected with RISQGPU_ERR_CAPACITY.
+ * Ordering: the call runs on the handle's stream, which by default does not wait
+ * for other streams.  x_dev must therefore be complete before the call, or the
+ * caller routes the handle onto the stream that produces x_dev with
+ * risqgpu_set_stream.  The call returns after its own work has finished.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress, with the handle's device current), so make that first
+ * call before any CUDA stream capture begins.  All calls share the array, so
+ * calls that overlap on the GPU (other handles or threads, other streams) race;
+ * the contents left by a previous call are never read. */
 RISQGPU_API int risqgpu_sigma_noalloc(risqgpu_t* h, const double* x_dev, double* y_dev);
 
 /* Element-level entry points (parity tests): H_ii and H_ij of dets[k] / (d1[k], d2[k]). */

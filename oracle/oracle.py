@@ -71,6 +71,16 @@ def lib():
         L.or_mgs.restype = C.c_int
         L.or_davidson.argtypes = [C.c_void_p, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _dp, _ip]
         L.or_davidson.restype = C.c_int
+        L.or_davidson_par.argtypes = [C.c_void_p, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _dp, _ip]
+        L.or_davidson_par.restype = C.c_int
+        L.or_sparse_build_par.argtypes = [C.c_void_p, C.c_void_p, _u64p, C.c_size_t, _dp]
+        L.or_sparse_build_par.restype = C.c_int
+        L.or_sparse_mv_par.argtypes = [C.c_void_p, _dp, _dp]
+        L.or_num_threads.restype = C.c_int
+        L.or_rows_bruteforce.argtypes = [C.c_void_p, _u64p, C.c_size_t, _i64p, C.c_size_t, _i64p, _i64p, _dp,
+                                         C.c_size_t]
+        L.or_rows_bruteforce.restype = C.c_int
+        L.or_hci_set_options.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.or_davidson_dense.argtypes = [_dp, C.c_size_t, C.c_int, _dp, C.c_double, C.c_double, C.c_int, _dp, _dp, _ip]
         L.or_davidson_dense.restype = C.c_int
         L.or_hci_new.restype = C.c_void_p
@@ -190,6 +200,20 @@ class Sparse:
             raise RuntimeError(f"oracle sparse build failed ({r})")
         return self
 
+    def build_par(self, ham: Ham, dets, diag):
+        """The fast builder's pairs and values for the whole set, on every host core."""
+        d = np.ascontiguousarray(dets, dtype=np.uint64)
+        dg = np.ascontiguousarray(diag, dtype=np.float64)
+        if lib().or_sparse_build_par(self.ptr, ham.ptr, _p(d, _u64p), d.shape[0], _p(dg, _dp)) != 0:
+            raise RuntimeError("oracle parallel build needs an empty matrix")
+        return self
+
+    def mv_par(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(self.n)
+        lib().or_sparse_mv_par(self.ptr, _p(x, _dp), _p(y, _dp))
+        return y
+
     @property
     def n(self):
         return lib().or_sparse_n(self.ptr)
@@ -214,7 +238,7 @@ class Sparse:
         lib().or_sparse_mv(self.ptr, _p(x, _dp), _p(y, _dp))
         return y
 
-    def davidson(self, nvalues=1, init=None, tol=1e-4, etol=1e-8, max_iters=50):
+    def davidson(self, nvalues=1, init=None, tol=1e-4, etol=1e-8, max_iters=50, parallel=False):
         n = self.n
         ev = np.zeros(nvalues)
         vec = np.zeros((nvalues, n))
@@ -223,13 +247,36 @@ class Sparse:
         if init is not None:
             init = np.ascontiguousarray(init, dtype=np.float64)
             ip = _p(init, _dp)
-        r = lib().or_davidson(self.ptr, nvalues, ip, tol, etol, max_iters, _p(ev, _dp), _p(vec, _dp), _p(st, _ip))
+        fn = lib().or_davidson_par if parallel else lib().or_davidson
+        r = fn(self.ptr, nvalues, ip, tol, etol, max_iters, _p(ev, _dp), _p(vec, _dp), _p(st, _ip))
         return r, ev, vec, dict(iters=int(st[0]), n_sigma=int(st[1]), converged=bool(st[2]), reason=int(st[3]))
 
     def __del__(self):
         if getattr(self, "ptr", None) and _lib is not None:
             _lib.or_sparse_free(self.ptr)
             self.ptr = None
+
+
+def rows_bruteforce(ham: Ham, dets, rows, cap=None):
+    """Full rows of the given determinants against the whole set by brute force: a list of
+    (cols, vals) per row, columns ascending (the fast builder's rule and values)."""
+    d = np.ascontiguousarray(dets, dtype=np.uint64)
+    r = np.ascontiguousarray(rows, dtype=np.int64)
+    if cap is None:
+        cap = 20000 * len(r) + 1
+    off = np.zeros(len(r) + 1, dtype=np.int64)
+    cols = np.zeros(cap, dtype=np.int64)
+    vals = np.zeros(cap)
+    rc = lib().or_rows_bruteforce(ham.ptr, _p(d, _u64p), d.shape[0], _p(r, _i64p), len(r), _p(off, _i64p),
+                                  _p(cols, _i64p), _p(vals, _dp), cap)
+    if rc != 0:
+        raise RuntimeError(f"row capacity {cap} too small ({off[-1]} entries)")
+    return [(cols[off[i]:off[i + 1]].copy(), vals[off[i]:off[i + 1]].copy()) for i in range(len(r))]
+
+
+def num_threads() -> int:
+    """Threads the oracle's multi-threaded paths use (OpenMP)."""
+    return lib().or_num_threads()
 
 
 def davidson_dense(A, nvalues=1, init=None, tol=1e-4, etol=1e-8, max_iters=50):
@@ -273,6 +320,12 @@ class Hci:
         self.ptr = lib().or_hci_new(ham.ptr, nup, ndn, z_sym, eps_var, builder, 1 if grouped_singles else 0)
         if not self.ptr:
             raise ValueError("unsupported HCI start")
+
+    def set_options(self, dav_max_iter=50, parallel=False):
+        """Davidson cap of each solve (the reference fixes 50) and the multi-threaded
+        build and sigma."""
+        lib().or_hci_set_options(self.ptr, int(dav_max_iter), 1 if parallel else 0)
+        return self
 
     def run(self, max_iter=20) -> float:
         return lib().or_hci_run(self.ptr, max_iter)

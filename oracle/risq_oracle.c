@@ -24,6 +24,9 @@
 #include <stdlib.h>
 #include <string.h>
 #include <errno.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 
 typedef unsigned __int128 u128;
 
@@ -1296,6 +1299,179 @@ OR_EXPORT int or_davidson(const Sparse *s, int nvalues, const double *init, doub
     return r;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Multi-threaded (OpenMP) fast build and sigma, for the CPU baseline on every  */
+/* host core.  The build produces the pairs and values of                       */
+/* gen_sparse_ham_fast_lookup with n_stored_h = 0 (fast_ham.rs:527-575): every   */
+/* pair i < j at excitation degree 1 or 2 is found once, by its row i, through   */
+/* the same alpha group, the same beta group, or an alpha single-partner group,  */
+/* and valued ham_off_diag_no_excite(det_i, det_j); singles are kept iff         */
+/* |H| > 1e-12 (fast_ham.rs:505,510), doubles iff H != 0 (off_diag.rs:33).  The  */
+/* serial builder computes the singles with the same argument order and the     */
+/* doubles are symmetric in their arguments, so the stored values are the same.  */
+/* sigma is matrix_vector_prod (sparse.rs:64-78) with the rows shared out        */
+/* round-robin between the threads, each thread scattering into its own copy of  */
+/* y; the copies are summed in thread order.                                     */
+/* ------------------------------------------------------------------------- */
+
+OR_EXPORT int or_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+OR_EXPORT int or_sparse_build_par(Sparse *s, const Ham *h, const uint64_t *dets, size_t N, const double *diag) {
+    if (s->n) return -1;
+    Config *cf = malloc(sizeof(Config) * (N ? N : 1));
+    for (size_t i = 0; i < N; i++) cf[i] = cfg_from(dets + 4 * i);
+    sparse_expand(s, N, diag);
+    Groups ga, gb;
+    groups_build(&ga, cf, N, 0);
+    groups_build(&gb, cf, N, 1);
+    Partners pa;
+    partners_build(&pa, &ga);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (size_t i = 0; i < N; i++) {
+        Row *r = &s->rows[i];
+        const Config ci = cf[i];
+        /* same alpha string: beta singles and beta-beta doubles */
+        size_t g = ga.gid[i];
+        for (size_t k = ga.start[g]; k < ga.start[g + 1]; k++) {
+            const size_t j = (size_t)ga.order[k];
+            if (j <= i) continue;
+            const int d = popc128(ci.dn ^ cf[j].dn);
+            if (d != 2 && d != 4) continue;
+            const double e = ham_off_diag_no_excite(h, ci, cf[j]);
+            if (d == 2 ? fabs(e) > 1e-12 : e != 0.0) row_push(r, (int64_t)j, e);
+        }
+        /* same beta string: alpha singles and alpha-alpha doubles */
+        g = gb.gid[i];
+        for (size_t k = gb.start[g]; k < gb.start[g + 1]; k++) {
+            const size_t j = (size_t)gb.order[k];
+            if (j <= i) continue;
+            const int d = popc128(ci.up ^ cf[j].up);
+            if (d != 2 && d != 4) continue;
+            const double e = ham_off_diag_no_excite(h, ci, cf[j]);
+            if (d == 2 ? fabs(e) > 1e-12 : e != 0.0) row_push(r, (int64_t)j, e);
+        }
+        /* opposite-spin doubles: alpha single partners whose beta differs by one electron */
+        const size_t a = ga.gid[i];
+        for (size_t pk = pa.start[a]; pk < pa.start[a + 1]; pk++) {
+            const size_t a2 = pa.part[pk];
+            for (size_t k = ga.start[a2]; k < ga.start[a2 + 1]; k++) {
+                const size_t j = (size_t)ga.order[k];
+                if (j <= i || popc128(ci.dn ^ cf[j].dn) != 2) continue;
+                const double e = ham_off_diag_no_excite(h, ci, cf[j]);
+                if (e != 0.0) row_push(r, (int64_t)j, e);
+            }
+        }
+        stable_sort_cols(r->e, r->n);
+        s->nnz[i] = r->n;
+    }
+    partners_free(&pa);
+    groups_free(&ga);
+    groups_free(&gb);
+    free(cf);
+    return 0;
+}
+
+/* Full rows of the sampled determinants against the whole set, by brute force (no
+ * lookup tables): for row r every j != r at excitation degree 1 or 2 whose element
+ * passes the fast builder's rule, valued as the fast builder values the pair
+ * (ham_off_diag_no_excite(det_min(r,j), det_max(r,j)), fast_ham.rs:473-517;
+ * off_diag.rs:26-39).  Entries of row rows[i] fill out_* from off[i], with
+ * off[k] = total; columns ascending within a row.  Returns 0, or -1 when the
+ * total exceeds cap (off[] is filled either way). */
+static int brute_row(const Ham *h, const Config *cf, size_t N, size_t r, int64_t *oc, double *ov) {
+    int n = 0;
+    const Config a = cf[r];
+    for (size_t j = 0; j < N; j++) {
+        if (j == r) continue;
+        const int du = popc128(a.up ^ cf[j].up), dd = popc128(a.dn ^ cf[j].dn);
+        const int d = du + dd;
+        if (d != 2 && d != 4) continue;
+        const double e = r < j ? ham_off_diag_no_excite(h, a, cf[j]) : ham_off_diag_no_excite(h, cf[j], a);
+        const int keep = d == 2 ? fabs(e) > 1e-12 : e != 0.0;
+        if (!keep) continue;
+        if (oc) { oc[n] = (int64_t)j; ov[n] = e; }
+        n++;
+    }
+    return n;
+}
+
+OR_EXPORT int or_rows_bruteforce(const Ham *h, const uint64_t *dets, size_t N, const int64_t *rows, size_t k,
+                                 int64_t *off, int64_t *out_c, double *out_v, size_t cap) {
+    Config *cf = malloc(sizeof(Config) * (N ? N : 1));
+    for (size_t i = 0; i < N; i++) cf[i] = cfg_from(dets + 4 * i);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (size_t i = 0; i < k; i++) off[i + 1] = brute_row(h, cf, N, (size_t)rows[i], NULL, NULL);
+    off[0] = 0;
+    for (size_t i = 0; i < k; i++) off[i + 1] += off[i];
+    int rc = (size_t)off[k] > cap ? -1 : 0;
+    if (rc == 0) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (size_t i = 0; i < k; i++) brute_row(h, cf, N, (size_t)rows[i], out_c + off[i], out_v + off[i]);
+    }
+    free(cf);
+    return rc;
+}
+
+typedef struct { const Sparse *s; double *buf; int nt; } ParCtx;
+
+static void sparse_mv_par(const void *ctx, const double *x, double *y) {
+    const ParCtx *c = ctx;
+    const Sparse *s = c->s;
+    const size_t n = s->n;
+#pragma omp parallel num_threads(c->nt)
+    {
+#ifdef _OPENMP
+        const int t = omp_get_thread_num();
+#else
+        const int t = 0;
+#endif
+        double *yt = c->buf + (size_t)t * n;
+        for (size_t i = 0; i < n; i++) yt[i] = 0.0;
+#pragma omp barrier
+#pragma omp for schedule(static, 64)
+        for (size_t i = 0; i < n; i++) {
+            const Row *r = &s->rows[i];
+            const double xi = x[i];
+            double acc = s->diag[i] * xi;
+            for (size_t k = 0; k < r->n; k++) {
+                acc += r->e[k].val * x[r->e[k].col];
+                yt[r->e[k].col] += r->e[k].val * xi;
+            }
+            yt[i] += acc;
+        }
+#pragma omp for schedule(static)
+        for (size_t i = 0; i < n; i++) {
+            double v = 0.0;
+            for (int u = 0; u < c->nt; u++) v += c->buf[(size_t)u * n + i];
+            y[i] = v;
+        }
+    }
+}
+
+OR_EXPORT void or_sparse_mv_par(const Sparse *s, const double *x, double *y) {
+    ParCtx c = {s, NULL, or_num_threads()};
+    c.buf = malloc(sizeof(double) * (size_t)c.nt * (s->n ? s->n : 1));
+    sparse_mv_par(&c, x, y);
+    free(c.buf);
+}
+
+OR_EXPORT int or_davidson_par(const Sparse *s, int nvalues, const double *init, double tol, double etol,
+                              int max_iters, double *evals, double *evecs, int *stats4) {
+    ParCtx c = {s, NULL, or_num_threads()};
+    c.buf = malloc(sizeof(double) * (size_t)c.nt * (s->n ? s->n : 1));
+    DavStats st = {0};
+    int r = davidson(&c, sparse_mv_par, s->diag, s->n, nvalues, init, tol, etol, max_iters, evals, evecs, &st);
+    if (stats4) { stats4[0] = st.iters; stats4[1] = st.n_sigma; stats4[2] = st.converged; stats4[3] = st.reason; }
+    free(c.buf);
+    return r;
+}
+
 /* Davidson over a dense symmetric matrix (row-major), used to pin the solver. */
 typedef struct { const double *A; size_t n; } DenseCtx;
 static void dense_mv_cb(const void *ctx, const double *x, double *y) {
@@ -1397,6 +1573,7 @@ typedef struct {
     Sparse *sp;
     int converged;
     int builder, grouped_singles;
+    int dav_max_iter, parallel;
     /* per-iteration log */
     int nlog;
     double log_eps[64], log_energy[64];
@@ -1503,7 +1680,17 @@ static void sparse_optimize(Hci *H, double coeff_eps, double energy_eps, int ini
     Config *cf = malloc(sizeof(Config) * N);
     double *diag = malloc(sizeof(double) * N);
     for (size_t i = 0; i < N; i++) { cf[i] = H->wf.dets[i].config; diag[i] = H->wf.dets[i].diag; }
-    sparse_build(H->sp, H->ham, cf, N, H->n_stored_h, diag, H->builder, H->grouped_singles);
+    if (H->parallel) {
+        /* every pair rebuilt on all cores (the fast builder's rule for the whole set) */
+        or_sparse_free(H->sp);
+        H->sp = or_sparse_new();
+        uint64_t *d4 = malloc(sizeof(uint64_t) * 4 * (N ? N : 1));
+        for (size_t i = 0; i < N; i++) cfg_to(cf[i], d4 + 4 * i);
+        or_sparse_build_par(H->sp, H->ham, d4, N, diag);
+        free(d4);
+    } else {
+        sparse_build(H->sp, H->ham, cf, N, H->n_stored_h, diag, H->builder, H->grouped_singles);
+    }
     H->n_stored_h = N;
     double *init = NULL;
     if (init_last_iter) {
@@ -1513,7 +1700,9 @@ static void sparse_optimize(Hci *H, double coeff_eps, double energy_eps, int ini
     double ev;
     double *evec = malloc(sizeof(double) * N);
     DavStats st = {0};
-    int r = davidson(H->sp, sparse_mv_cb, H->sp->diag, N, 1, init, coeff_eps, energy_eps, 50, &ev, evec, &st);
+    int r;
+    if (H->parallel) r = or_davidson_par(H->sp, 1, init, coeff_eps, energy_eps, H->dav_max_iter, &ev, evec, NULL);
+    else r = davidson(H->sp, sparse_mv_cb, H->sp->diag, N, 1, init, coeff_eps, energy_eps, H->dav_max_iter, &ev, evec, &st);
     if (r == 0) {
         H->wf.energy = ev;
         for (size_t i = 0; i < N; i++) H->wf.dets[i].coeff = evec[i];
@@ -1544,7 +1733,15 @@ OR_EXPORT Hci *or_hci_new(const Ham *h, int nup, int ndn, int z_sym, double eps_
     H->eps_iter = init_eps(&H->wf, eps_var, z_sym, H->eg);
     H->sp = or_sparse_new();
     H->n_stored_h = 0;
+    H->dav_max_iter = 50; /* Config::new, algorithms/davidson.rs:73 */
     return H;
+}
+
+/* Davidson iteration cap of each solve (the reference fixes 50) and the
+ * multi-threaded build / sigma (0 = the serial restatement). */
+OR_EXPORT void or_hci_set_options(Hci *H, int dav_max_iter, int parallel) {
+    H->dav_max_iter = dav_max_iter > 0 ? dav_max_iter : 50;
+    H->parallel = parallel;
 }
 
 OR_EXPORT void or_hci_free(Hci *H) {

@@ -36,7 +36,8 @@ class HStats(C.Structure):
     _fields_ = [("n_dets", C.c_uint64), ("nnz_upper", C.c_uint64), ("nnz_full", C.c_uint64),
                 ("candidates", C.c_uint64), ("ms_setup", C.c_double), ("ms_count", C.c_double),
                 ("ms_fill", C.c_double), ("ms_total", C.c_double), ("bytes_csr", C.c_uint64),
-                ("gpu_ms_count", C.c_double), ("gpu_ms_fill", C.c_double)]
+                ("gpu_ms_count", C.c_double), ("gpu_ms_fill", C.c_double), ("n_tiles", C.c_uint64),
+                ("nnz_dense", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -80,12 +81,17 @@ SIGNATURES = [
     ("risqgpu_build_h", C.c_int, [_handle, C.c_int, C.c_int, C.POINTER(HStats)]),
     ("risqgpu_nnz", C.c_int, [_handle, _u64p, _u64p]),
     ("risqgpu_export_upper", C.c_int, [_handle, _i64p, _i64p, _dp, C.c_size_t, _dp]),
+    ("risqgpu_export_rows", C.c_int, [_handle, _i64p, C.c_size_t, _i64p, _i64p, _dp, C.c_size_t,
+                                      C.POINTER(C.c_size_t)]),
     ("risqgpu_sigma", C.c_int, [_handle, _dp, _dp, C.c_int]),
     ("risqgpu_sigma_device", C.c_int, [_handle, C.c_void_p, C.c_void_p, C.c_int]),
     ("risqgpu_davidson", C.c_int, [_handle, C.c_int, _dp, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int,
                                    _dp, _dp, C.POINTER(DStats)]),
     ("risqgpu_sparse_optimize", C.c_int, [_handle, _dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                           _dp, _dp, C.POINTER(HStats), C.POINTER(DStats)]),
+    ("risqgpu_set_subspace", C.c_int, [_handle, C.c_int, C.c_int]),
+    ("risqgpu_set_memory_limit", C.c_int, [_handle, C.c_size_t]),
+    ("risqgpu_memory_used", C.c_int, [_handle, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("risqgpu_set_stream", C.c_int, [_handle, C.c_void_p]),
     ("risqgpu_sigma_noalloc", C.c_int, [_handle, C.c_void_p, C.c_void_p]),
     ("risqgpu_ham_diag", C.c_int, [_handle, _u64p, C.c_size_t, _dp]),

@@ -15,10 +15,13 @@
 //   (1) its alpha group            -> beta singles and beta-beta doubles
 //   (2) its beta group             -> alpha singles and alpha-alpha doubles
 //   (3) its alpha-partner groups   -> opposite-spin doubles (beta differs by one)
-// The matrix is held with both triangles (each element is computed once per
-// side; ham_sing/ham_doub are bitwise symmetric, see bits.cuh) so sigma needs no
-// scatter.  One warp builds one row: a count pass sizes the rows, a fill pass
-// evaluates FP64 Slater-Condon and compacts the non-zeros with warp ballots.
+// The matrix is held either with both triangles (each element computed once per
+// side; ham_sing/ham_doub are bitwise symmetric, see bits.cuh), so that every sigma
+// output is a private row sum, or as the upper triangle only (each pair once, the
+// reference's SparseMatUpperTri), regrouped into row-panel x column-window tiles
+// for sigma (tiles.cu).  One warp builds one row: a count pass sizes the rows, a
+// fill pass evaluates FP64 Slater-Condon and compacts the non-zeros with warp
+// ballots.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -296,7 +299,8 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
                                                     int64_t* __restrict__ cnt, const int64_t* __restrict__ row_start,
                                                     int32_t* __restrict__ row_len, int32_t* __restrict__ cols,
                                                     double* __restrict__ v64, float* __restrict__ v32,
-                                                    float* __restrict__ vlo) {
+                                                    float* __restrict__ vlo, int64_t row_lo, int64_t row_hi,
+                                                    int64_t base_off) {
     constexpr int WARPS = 256 / 32;
     constexpr int QCAP = 64;  // < 32 pending + 32 new
     __shared__ int s_q[WARPS][2][QCAP];
@@ -310,12 +314,12 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
     unsigned char* const kd = s_k[wib][1];
     for (;;) {
         int p = 0;
-        if (lane == 0) p = atomicAdd(row_counter, 1);
+        if (lane == 0) p = (int)row_lo + atomicAdd(row_counter, 1);
         p = __shfl_sync(FULL, p, 0);
-        if (p >= v.N) break;
+        if (p >= row_hi) break;
         const Bits<W> a = v.up_at(p), b = v.dn_at(p);
         const bool p_new = v.nsh == 0 || v.orig[p] >= v.nsh;
-        int64_t base = MODE ? row_start[p] : 0;
+        int64_t base = MODE ? row_start[p] - base_off : 0;
         int count = 0;
         int ns = 0, nd = 0;  // queue fill, warp-uniform
 
@@ -819,19 +823,184 @@ __global__ void k_invert(const int32_t* __restrict__ orig, int64_t n, int32_t* _
 }
 
 template <int W>
+int launch_fill(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int upper, int precision, int* counter,
+                int blocks, int threads, int32_t* cols, double* v64, float* v32, float* vlo, int64_t row_lo,
+                int64_t row_hi, int64_t base) {
+    if (precision == RISQGPU_FP64)
+        k_build_rows<W, 1><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start,
+                                                              h->d_row_len, cols, v64, nullptr, nullptr, row_lo,
+                                                              row_hi, base);
+    else if (precision == RISQGPU_FP32)
+        k_build_rows<W, 2><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start,
+                                                              h->d_row_len, cols, nullptr, v32, nullptr, row_lo,
+                                                              row_hi, base);
+    else if (precision == RISQGPU_MIXED)
+        k_build_rows<W, 3><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start,
+                                                              h->d_row_len, cols, nullptr, v32, vlo, row_lo, row_hi,
+                                                              base);
+    else
+        k_build_rows<W, 4><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start,
+                                                              h->d_row_len, cols, nullptr, nullptr, nullptr, row_lo,
+                                                              row_hi, base);
+    return check_launch(h, "fill rows");
+}
+
+__global__ void k_panel_starts(const int64_t* __restrict__ row_start, int64_t n, int rb, int64_t np,
+                               int64_t* __restrict__ out) {
+    for (int64_t P = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; P <= np; P += (int64_t)gridDim.x * blockDim.x)
+        out[P] = row_start[min(n, P << rb)];
+}
+
+// Upper-triangle fill through the tiled layout: the rows are filled chunk by chunk of
+// whole panels into a CSR buffer that holds one chunk, and every chunk is regrouped
+// into tiles before the next is filled, so that the device holds the tiled arrays
+// plus one chunk rather than two copies of the matrix.
+template <int W>
+int fill_tiled(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int precision, int* counter, int64_t cap,
+               int blocks, int threads) {
+    const int64_t n = (int64_t)h->N;
+    int rb = 0, cb = 0;
+    if (tile_shape(n, rb, cb) != RISQGPU_OK) {
+        h->err = "determinant set too large for the tiled upper-triangle layout";
+        return RISQGPU_ERR_INVALID;
+    }
+    h->tile_rb = rb;
+    h->tile_cb = cb;
+    const int64_t np = (n + ((int64_t)1 << rb) - 1) >> rb;
+    std::vector<int64_t> ps((size_t)np + 1);
+    {
+        int64_t* dps = nullptr;
+        ScopedFree<1> release(dps);
+        RQ_TRY(dalloc(h, dps, (size_t)np + 1));
+        k_panel_starts<<<grid_for(h, np + 1), 256, 0, h->stream>>>(h->d_row_start, n, rb, np, dps);
+        RQ_CUDA(h, cudaMemcpyAsync(ps.data(), dps, sizeof(int64_t) * (np + 1), cudaMemcpyDeviceToHost, h->stream));
+        RQ_TRY(sync(h, "panel starts"));
+    }
+    const size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_MIXED ? 8 : 4);
+    const size_t per_el = 4 + vb;
+    // bytes held besides the element arrays: per-row tile data, accumulators, margin
+    const size_t fixed = (size_t)cap * per_el + (size_t)n * 32 + ((size_t)256 << 20);
+    const size_t avail = mem_available(h);
+    // chunks: the fewest whose largest chunk fits beside the tiled arrays
+    std::vector<int64_t> cuts;
+    int64_t max_chunk = 0;
+    for (int64_t K = 1;; K = K < 8 ? K + 1 : K * 2) {
+        const int64_t target = (cap + K - 1) / K;
+        cuts.assign(1, 0);
+        max_chunk = 0;
+        int64_t start = 0;
+        for (int64_t P = 1; P <= np; P++) {
+            const bool last = P == np;
+            if (last || ps[P + 1] - ps[start] > target) {
+                if (!last && P == start) continue;
+                cuts.push_back(P);
+                max_chunk = std::max(max_chunk, ps[P] - ps[start]);
+                start = P;
+            }
+        }
+        if (fixed + (size_t)max_chunk * per_el <= avail) break;
+        if (K >= np) {
+            h->err = "tiled upper-triangle H needs " + std::to_string((fixed + (size_t)max_chunk * per_el) >> 20) +
+                     " MiB, " + std::to_string(avail >> 20) + " MiB available";
+            return RISQGPU_ERR_OOM;
+        }
+    }
+    int32_t* ccols = nullptr;
+    double* c64 = nullptr;
+    float *c32 = nullptr, *clo = nullptr;
+    ScopedFree<4> release(ccols, c64, c32, clo);
+    RQ_TRY(dalloc(h, h->d_el_idx, (size_t)cap));
+    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, (size_t)cap));
+    else RQ_TRY(dalloc(h, h->d_val32, (size_t)cap));
+    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, (size_t)cap));
+    RQ_TRY(dalloc(h, ccols, (size_t)max_chunk));
+    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, c64, (size_t)max_chunk));
+    else RQ_TRY(dalloc(h, c32, (size_t)max_chunk));
+    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, clo, (size_t)max_chunk));
+    TileBuilder tb;
+    RQ_TRY(tb.begin(h, np));
+    for (size_t c = 0; c + 1 < cuts.size(); c++) {
+        const int64_t p_lo = cuts[c], p_hi = cuts[c + 1];
+        const int64_t r_lo = p_lo << rb, r_hi = std::min(n, p_hi << rb);
+        const int64_t base = ps[p_lo];
+        RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
+        RQ_TRY(launch_fill<W>(h, v, I, thr, 1, precision, counter, blocks, threads, ccols, c64, c32, clo, r_lo, r_hi,
+                              base));
+        if (precision == RISQGPU_FP64)
+            RQ_TRY(tb.chunk<double>(p_lo, p_hi, h->d_row_start, base, h->d_row_len, ccols, c64, nullptr, h->d_val64,
+                                    nullptr));
+        else
+            RQ_TRY(tb.chunk<float>(p_lo, p_hi, h->d_row_start, base, h->d_row_len, ccols, c32, clo, h->d_val32,
+                                   h->d_val_lo));
+    }
+    return tb.finish();
+}
+
+// stored count, statistics and handle state after a fill
+int finish_build(risqgpu* h, int precision, int upper, int64_t cap, std::chrono::steady_clock::time_point t0,
+                 std::chrono::steady_clock::time_point t1, std::chrono::steady_clock::time_point t2, cudaEvent_t* ev,
+                 risqgpu_hstats* st) {
+    using clk = std::chrono::steady_clock;
+    const int64_t n = (int64_t)h->N;
+    int64_t* sum = nullptr;
+    char* tmp = nullptr;
+    ScopedFree<2> release(sum, tmp);
+    RQ_TRY(dalloc(h, sum, 1));
+    size_t tb = 0;
+    cub::DeviceReduce::Sum(nullptr, tb, h->d_row_len, sum, (int)n, h->stream);
+    RQ_TRY(dalloc(h, tmp, tb));
+    cub::DeviceReduce::Sum(tmp, tb, h->d_row_len, sum, (int)n, h->stream);
+    RQ_TRY(sync(h, "fill rows"));
+    auto t3 = clk::now();
+    int64_t nnz = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&nnz, sum, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "nnz"));
+    h->cap = (size_t)cap;
+    h->nnz_full = upper ? 2 * (uint64_t)nnz : (uint64_t)nnz;
+    h->nnz_upper = upper ? (uint64_t)nnz : (uint64_t)nnz / 2;
+    h->precision = precision;
+    h->upper = upper != 0;
+    float ms_c = 0.f, ms_f = 0.f;
+    cudaEventElapsedTime(&ms_c, ev[0], ev[1]);
+    cudaEventElapsedTime(&ms_f, ev[2], ev[3]);
+    if (st) {
+        st->gpu_ms_count = ms_c;
+        st->gpu_ms_fill = ms_f;
+        st->candidates = (uint64_t)cap;
+        st->ms_count = std::chrono::duration<double, std::milli>(t1 - t0).count();
+        st->ms_fill = std::chrono::duration<double, std::milli>(t3 - t2).count();
+        size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : (precision == RISQGPU_COLS ? 0 : 8));
+        st->bytes_csr = (uint64_t)nnz * (4 + vb);
+        st->n_tiles = (uint64_t)h->n_tiles;
+        st->nnz_dense = h->n_dense_el;
+    }
+    return RISQGPU_OK;
+}
+
+// Destroys the build's timing events on every exit.
+struct BuildEvents {
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    ~BuildEvents() {
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
+
+template <int W>
 int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats* st) {
     using clk = std::chrono::steady_clock;
     const int64_t n = (int64_t)h->N;
     const bool incremental = h->nsh > 0 && h->d_prev_row_start != nullptr;
     int32_t* prev_inv = nullptr;
+    int* counter = nullptr;
+    int64_t* cnt = nullptr;
+    ScopedFree<3> release(prev_inv, counter, cnt);
     if (incremental) {
         RQ_TRY(dalloc(h, prev_inv, h->prev_N));
         k_invert<<<grid_for(h, h->prev_N), 256, 0, h->stream>>>(h->d_prev_orig, (int64_t)h->prev_N, prev_inv);
     }
     SetView<W> v = make_view<W>(h, incremental, prev_inv);
     Ints I{h->d_h1, h->d_h2, h->nuc};
-    int* counter = nullptr;
-    int64_t* cnt = nullptr;
     RQ_TRY(dalloc(h, counter, 1));
     RQ_TRY(dalloc(h, cnt, n + 1));
     RQ_TRY(dalloc(h, h->d_row_start, n + 1));
@@ -842,55 +1011,50 @@ int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats*
     const int blocks = num_sms(h) * std::max(occ, 1);
 
     RQ_TRY(sync(h, "pre-count"));
-    cudaEvent_t ev[4];
-    for (auto& e : ev) RQ_CUDA(h, cudaEventCreate(&e));
+    BuildEvents be;
+    cudaEvent_t* ev = be.ev;
+    for (int k = 0; k < 4; k++) RQ_CUDA(h, cudaEventCreate(&ev[k]));
     auto t0 = clk::now();
     RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
     RQ_CUDA(h, cudaEventRecord(ev[0], h->stream));
-    k_build_rows<W, 0><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, cnt, nullptr, nullptr, nullptr, nullptr,
-                                                          nullptr, nullptr);
+    k_build_rows<W, 0><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, cnt, nullptr, nullptr, nullptr,
+                                                          nullptr, nullptr, nullptr, 0, n, 0);
     RQ_CUDA(h, cudaEventRecord(ev[1], h->stream));
     RQ_TRY(check_launch(h, "count rows"));
     {
         size_t tb = 0;
         cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt, h->d_row_start, (int)(n + 1), h->stream);
         char* tmp = nullptr;
+        ScopedFree<1> release_tmp(tmp);
         RQ_TRY(dalloc(h, tmp, tb));
         RQ_CUDA(h, cudaMemsetAsync(cnt + n, 0, sizeof(int64_t), h->stream));
         cub::DeviceScan::ExclusiveSum(tmp, tb, cnt, h->d_row_start, (int)(n + 1), h->stream);
         RQ_TRY(sync(h, "row scan"));
-        dfree(tmp);
     }
     int64_t cap = 0;
     RQ_CUDA(h, cudaMemcpyAsync(&cap, h->d_row_start + n, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
     RQ_TRY(sync(h, "count rows"));
+    dfree(cnt);
     auto t1 = clk::now();
+    if (upper) {
+        // upper-triangle storage: filled chunk by chunk and regrouped into tiles
+        auto t2 = clk::now();
+        RQ_CUDA(h, cudaEventRecord(ev[2], h->stream));
+        RQ_TRY(fill_tiled<W>(h, v, I, thr, precision, counter, cap, blocks, threads));
+        RQ_CUDA(h, cudaEventRecord(ev[3], h->stream));
+        return finish_build(h, precision, upper, cap, t0, t1, t2, ev, st);
+    }
     {
         // refuse up front when the rows cannot be stored, leaving the handle unchanged
         size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : (precision == RISQGPU_COLS ? 0 : 8));
         size_t need = (size_t)cap * (4 + vb) + ((size_t)64 << 20);
-        size_t fr = 0, tot = 0;
-        RQ_CUDA(h, cudaMemGetInfo(&fr, &tot));
-        // the current column and value arrays are released before the new ones are made
-        size_t held = 0;
-        if (h->d_cols) held += h->cap * sizeof(int32_t);
-        if (h->d_val64) held += h->cap * sizeof(double);
-        if (h->d_val32) held += h->cap * sizeof(float);
-        if (h->d_val_lo) held += h->cap * sizeof(float);
-        fr += held;
+        const size_t fr = mem_available(h);
         if (need > fr) {
             h->err = "sparse H needs " + std::to_string(need >> 20) + " MiB, " + std::to_string(fr >> 20) +
-                     " MiB free";
-            dfree(counter);
-            dfree(cnt);
-            dfree(prev_inv);
+                     " MiB available";
             return RISQGPU_ERR_OOM;
         }
     }
-    h->cap = (size_t)cap;
-    dfree(h->d_val64);
-    dfree(h->d_val32);
-    dfree(h->d_val_lo);
     RQ_TRY(dalloc(h, h->d_cols, cap));
     if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, cap));
     else if (precision != RISQGPU_COLS) RQ_TRY(dalloc(h, h->d_val32, cap));
@@ -899,58 +1063,10 @@ int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats*
     auto t2 = clk::now();
     RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
     RQ_CUDA(h, cudaEventRecord(ev[2], h->stream));
-    if (precision == RISQGPU_FP64)
-        k_build_rows<W, 1><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start, h->d_row_len,
-                                                              h->d_cols, h->d_val64, nullptr, nullptr);
-    else if (precision == RISQGPU_FP32)
-        k_build_rows<W, 2><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start, h->d_row_len,
-                                                              h->d_cols, nullptr, h->d_val32, nullptr);
-    else if (precision == RISQGPU_MIXED)
-        k_build_rows<W, 3><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start, h->d_row_len,
-                                                              h->d_cols, nullptr, h->d_val32, h->d_val_lo);
-    else
-        k_build_rows<W, 4><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start, h->d_row_len,
-                                                              h->d_cols, nullptr, nullptr, nullptr);
+    RQ_TRY(launch_fill<W>(h, v, I, thr, upper, precision, counter, blocks, threads, h->d_cols, h->d_val64, h->d_val32,
+                          h->d_val_lo, 0, n, 0));
     RQ_CUDA(h, cudaEventRecord(ev[3], h->stream));
-    RQ_TRY(check_launch(h, "fill rows"));
-    // stored count
-    int64_t* sum = nullptr;
-    RQ_TRY(dalloc(h, sum, 1));
-    {
-        size_t tb = 0;
-        cub::DeviceReduce::Sum(nullptr, tb, h->d_row_len, sum, (int)n, h->stream);
-        char* tmp = nullptr;
-        RQ_TRY(dalloc(h, tmp, tb));
-        cub::DeviceReduce::Sum(tmp, tb, h->d_row_len, sum, (int)n, h->stream);
-        RQ_TRY(sync(h, "fill rows"));
-        dfree(tmp);
-    }
-    auto t3 = clk::now();
-    int64_t nnz = 0;
-    RQ_CUDA(h, cudaMemcpyAsync(&nnz, sum, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
-    RQ_TRY(sync(h, "nnz"));
-    dfree(sum);
-    dfree(counter);
-    dfree(cnt);
-    dfree(prev_inv);
-    h->nnz_full = upper ? 2 * (uint64_t)nnz : (uint64_t)nnz;
-    h->nnz_upper = upper ? (uint64_t)nnz : (uint64_t)nnz / 2;
-    h->precision = precision;
-    h->upper = upper != 0;
-    float ms_c = 0.f, ms_f = 0.f;
-    cudaEventElapsedTime(&ms_c, ev[0], ev[1]);
-    cudaEventElapsedTime(&ms_f, ev[2], ev[3]);
-    for (auto& e : ev) cudaEventDestroy(e);
-    if (st) {
-        st->gpu_ms_count = ms_c;
-        st->gpu_ms_fill = ms_f;
-        st->candidates = (uint64_t)cap;
-        st->ms_count = std::chrono::duration<double, std::milli>(t1 - t0).count();
-        st->ms_fill = std::chrono::duration<double, std::milli>(t3 - t2).count();
-        size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : (precision == RISQGPU_COLS ? 0 : 8));
-        st->bytes_csr = (uint64_t)nnz * (4 + vb);
-    }
-    return RISQGPU_OK;
+    return finish_build(h, precision, upper, cap, t0, t1, t2, ev, st);
 }
 
 }  // namespace
@@ -958,6 +1074,7 @@ int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats*
 void free_csr(risqgpu* h) {
     dfree(h->d_row_start); dfree(h->d_row_len); dfree(h->d_cols);
     dfree(h->d_val64); dfree(h->d_val32); dfree(h->d_val_lo);
+    free_tiles(h);
     h->built = false;
     h->cap = 0;
     h->nnz_full = h->nnz_upper = 0;
@@ -1113,6 +1230,44 @@ int export_upper_impl(risqgpu* h, int64_t* rowptr, int64_t* cols, double* vals, 
     std::vector<int64_t> rs(n + 1);
     std::vector<int32_t> rl(n), ci(h->cap), orig(n);
     std::vector<double> v(h->cap);
+    if (h->tiled) {
+        // tiled storage: decode every pair to (p, q, value), then present it as rows of
+        // consecutive elements (row_start / row_len over the decoded order, sorted by p)
+        const size_t nz = h->nnz_upper;
+        int32_t *dp = nullptr, *dq = nullptr;
+        double* dv = nullptr;
+        ScopedFree<3> release(dp, dq, dv);
+        RQ_TRY(dalloc(h, dp, nz));
+        RQ_TRY(dalloc(h, dq, nz));
+        RQ_TRY(dalloc(h, dv, nz));
+        RQ_TRY(tiles_coo(h, dp, dq, dv));
+        RQ_TRY(sync(h, "tiled pairs"));
+        std::vector<int32_t> hp(nz);
+        ci.resize(nz);
+        v.resize(nz);
+        RQ_CUDA(h, cudaMemcpy(hp.data(), dp, sizeof(int32_t) * nz, cudaMemcpyDeviceToHost));
+        RQ_CUDA(h, cudaMemcpy(ci.data(), dq, sizeof(int32_t) * nz, cudaMemcpyDeviceToHost));
+        RQ_CUDA(h, cudaMemcpy(v.data(), dv, sizeof(double) * nz, cudaMemcpyDeviceToHost));
+        std::vector<int64_t> cnt(n + 1, 0);
+        for (size_t k = 0; k < nz; k++) cnt[hp[k] + 1]++;
+        for (size_t p = 0; p < n; p++) cnt[p + 1] += cnt[p];
+        std::vector<int32_t> c2(nz);
+        std::vector<double> v2(nz);
+        std::vector<int64_t> fill(cnt.begin(), cnt.end() - 1);
+        for (size_t k = 0; k < nz; k++) {
+            const int64_t at = fill[hp[k]]++;
+            c2[at] = ci[k];
+            v2[at] = v[k];
+        }
+        ci.swap(c2);
+        v.swap(v2);
+        for (size_t p = 0; p < n; p++) {
+            rs[p] = cnt[p];
+            rl[p] = (int32_t)(cnt[p + 1] - cnt[p]);
+        }
+        rs[n] = cnt[n];
+        RQ_CUDA(h, cudaMemcpy(orig.data(), h->d_orig, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    } else {
     RQ_CUDA(h, cudaMemcpy(rs.data(), h->d_row_start, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToHost));
     RQ_CUDA(h, cudaMemcpy(rl.data(), h->d_row_len, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
     RQ_CUDA(h, cudaMemcpy(ci.data(), h->d_cols, sizeof(int32_t) * h->cap, cudaMemcpyDeviceToHost));
@@ -1141,6 +1296,7 @@ int export_upper_impl(risqgpu* h, int64_t* rowptr, int64_t* cols, double* vals, 
             RQ_CUDA(h, cudaMemcpy(lo.data(), h->d_val_lo, sizeof(float) * h->cap, cudaMemcpyDeviceToHost));
         }
         for (size_t k = 0; k < h->cap; k++) v[k] = (double)hi[k] + (lo.empty() ? 0.0 : (double)lo[k]);
+    }
     }
     // count per caller row
     // full rows hold each pair twice (keep the caller-order upper one); upper storage
@@ -1180,6 +1336,96 @@ int export_upper_impl(risqgpu* h, int64_t* rowptr, int64_t* cols, double* vals, 
         RQ_CUDA(h, cudaMemcpy(dg.data(), h->d_diag, sizeof(double) * n, cudaMemcpyDeviceToHost));
         for (size_t p = 0; p < n; p++) diag[orig[p]] = dg[p];
     }
+    return RISQGPU_OK;
+}
+
+namespace {
+
+__global__ void k_mark_rows(const int64_t* __restrict__ rows, int64_t k, const int32_t* __restrict__ inv,
+                            uint32_t* __restrict__ mark) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < k; i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t p = inv[rows[i]];
+        atomicOr(mark + (p >> 5), 1u << (p & 31));
+    }
+}
+
+// full-row storage: the marked rows hold every element of themselves
+template <typename V, bool VLO>
+__global__ void k_rows_full(const int64_t* __restrict__ rows, int64_t k, const int32_t* __restrict__ inv,
+                            const int32_t* __restrict__ orig, const int64_t* __restrict__ row_start,
+                            const int32_t* __restrict__ row_len, const int32_t* __restrict__ cols,
+                            const V* __restrict__ vals, const float* __restrict__ vlo, int64_t* __restrict__ out_r,
+                            int64_t* __restrict__ out_c, double* __restrict__ out_v,
+                            unsigned long long* __restrict__ count, unsigned long long cap) {
+    for (int64_t i = blockIdx.x; i < k; i += gridDim.x) {
+        const int32_t p = inv[rows[i]];
+        const int64_t s = row_start[p];
+        for (int t = threadIdx.x; t < row_len[p]; t += blockDim.x) {
+            double v = (double)vals[s + t];
+            if constexpr (VLO) v += (double)vlo[s + t];
+            const unsigned long long at = atomicAdd(count, 1ull);
+            if (at < cap) {
+                out_r[at] = rows[i];
+                out_c[at] = orig[cols[s + t]];
+                out_v[at] = v;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int export_rows_impl(risqgpu* h, const int64_t* rows, size_t k, int64_t* out_r, int64_t* out_c, double* out_v,
+                     size_t cap, size_t* count) {
+    if (!h->built) { h->err = "no built matrix"; return RISQGPU_ERR_INVALID; }
+    if (h->precision == RISQGPU_COLS) { h->err = "row export needs stored values (not COLS)"; return RISQGPU_ERR_INVALID; }
+    for (size_t i = 0; i < k; i++)
+        if (rows[i] < 0 || (size_t)rows[i] >= h->N) { h->err = "row index out of range"; return RISQGPU_ERR_INVALID; }
+    // rows must be distinct (each is exported once per stored element)
+    {
+        std::vector<int64_t> sr(rows, rows + k);
+        std::sort(sr.begin(), sr.end());
+        if (std::adjacent_find(sr.begin(), sr.end()) != sr.end()) { h->err = "repeated row index"; return RISQGPU_ERR_INVALID; }
+    }
+    const int64_t n = (int64_t)h->N;
+    int64_t *drows = nullptr, *dr = nullptr, *dc = nullptr;
+    double* dv = nullptr;
+    uint32_t* mark = nullptr;
+    unsigned long long* cnt = nullptr;
+    ScopedFree<6> release(drows, dr, dc, dv, mark, cnt);
+    RQ_TRY(dalloc(h, drows, k));
+    RQ_TRY(dalloc(h, dr, cap));
+    RQ_TRY(dalloc(h, dc, cap));
+    RQ_TRY(dalloc(h, dv, cap));
+    RQ_TRY(dalloc(h, mark, (size_t)(n + 31) / 32));
+    RQ_TRY(dalloc(h, cnt, 1));
+    RQ_CUDA(h, cudaMemcpyAsync(drows, rows, sizeof(int64_t) * k, cudaMemcpyHostToDevice, h->stream));
+    RQ_CUDA(h, cudaMemsetAsync(mark, 0, sizeof(uint32_t) * ((n + 31) / 32), h->stream));
+    RQ_CUDA(h, cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), h->stream));
+    if (h->tiled) {
+        k_mark_rows<<<grid_for(h, (int64_t)k), 256, 0, h->stream>>>(drows, (int64_t)k, h->d_inv, mark);
+        RQ_TRY(tiles_rows(h, mark, dr, dc, dv, cnt, cap));
+    } else {
+        const int g = (int)std::max<size_t>(1, std::min<size_t>(k, 4096));
+        if (h->precision == RISQGPU_FP64)
+            k_rows_full<double, false><<<g, 256, 0, h->stream>>>(drows, (int64_t)k, h->d_inv, h->d_orig, h->d_row_start,
+                h->d_row_len, h->d_cols, h->d_val64, nullptr, dr, dc, dv, cnt, cap);
+        else if (h->precision == RISQGPU_MIXED)
+            k_rows_full<float, true><<<g, 256, 0, h->stream>>>(drows, (int64_t)k, h->d_inv, h->d_orig, h->d_row_start,
+                h->d_row_len, h->d_cols, h->d_val32, h->d_val_lo, dr, dc, dv, cnt, cap);
+        else
+            k_rows_full<float, false><<<g, 256, 0, h->stream>>>(drows, (int64_t)k, h->d_inv, h->d_orig, h->d_row_start,
+                h->d_row_len, h->d_cols, h->d_val32, nullptr, dr, dc, dv, cnt, cap);
+        RQ_TRY(check_launch(h, "row export"));
+    }
+    unsigned long long c = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&c, cnt, sizeof(c), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "row export"));
+    *count = (size_t)c;
+    if (c > cap) { h->err = "row export capacity too small: " + std::to_string(c) + " entries"; return RISQGPU_ERR_CAPACITY; }
+    RQ_CUDA(h, cudaMemcpy(out_r, dr, sizeof(int64_t) * c, cudaMemcpyDeviceToHost));
+    RQ_CUDA(h, cudaMemcpy(out_c, dc, sizeof(int64_t) * c, cudaMemcpyDeviceToHost));
+    RQ_CUDA(h, cudaMemcpy(out_v, dv, sizeof(double) * c, cudaMemcpyDeviceToHost));
     return RISQGPU_OK;
 }
 

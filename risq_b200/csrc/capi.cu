@@ -1,8 +1,34 @@
 // extern "C" entry points of librisqgpu.so (declared in include/risqgpu.h).
+#include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
+#include <unordered_map>
 
 #include "internal.cuh"
+
+namespace risq {
+
+namespace {
+std::mutex g_ledger_mu;
+std::unordered_map<void*, std::pair<risqgpu*, size_t>> g_ledger;
+}  // namespace
+
+void mem_record(risqgpu* h, void* p, size_t bytes) {
+    std::lock_guard<std::mutex> lk(g_ledger_mu);
+    g_ledger[p] = {h, bytes};
+    h->mem_used += bytes;
+}
+
+void mem_forget(void* p) {
+    std::lock_guard<std::mutex> lk(g_ledger_mu);
+    auto it = g_ledger.find(p);
+    if (it == g_ledger.end()) return;
+    it->second.first->mem_used -= it->second.second;
+    g_ledger.erase(it);
+}
+
+}  // namespace risq
 
 using namespace risq;
 
@@ -123,9 +149,25 @@ int risqgpu_export_upper(risqgpu_t* h, int64_t* rowptr, int64_t* cols, double* v
     return export_upper_impl(h, rowptr, cols, vals, cap, diag);
 }
 
+int risqgpu_export_rows(risqgpu_t* h, const int64_t* rows, size_t k, int64_t* out_row, int64_t* out_col,
+                        double* out_val, size_t cap, size_t* count) {
+    if (!h || !count || (k && !rows) || (cap && (!out_row || !out_col || !out_val))) return RISQGPU_ERR_INVALID;
+    DeviceGuard g(h->device);
+    *count = 0;
+    return export_rows_impl(h, rows, k, out_row, out_col, out_val, cap, count);
+}
+
 int risqgpu_sigma(risqgpu_t* h, const double* x, double* y, int nvec) {
     if (!h || !x || !y) return RISQGPU_ERR_INVALID;
     DeviceGuard g(h->device);
+    if (nvec >= 1 && h->built) {
+        const size_t n = h->N * (size_t)nvec;
+        for (size_t i = 0; i < n; i++)
+            if (!std::isfinite(x[i])) {
+                h->err = "x holds a non-finite value at index " + std::to_string(i);
+                return RISQGPU_ERR_INVALID;
+            }
+    }
     return sigma_host(h, x, y, nvec);
 }
 
@@ -166,6 +208,29 @@ int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs, double coef
     if (rc) return rc;
     *energy = e;
     std::memcpy(coeffs, v.data(), sizeof(double) * h->N);
+    return RISQGPU_OK;
+}
+
+int risqgpu_set_subspace(risqgpu_t* h, int max_space, int keep) {
+    if (!h || max_space < 0 || keep < 0 || max_space > 56 || (max_space > 0 && keep > max_space / 2)) {
+        if (h) h->err = "max_space must lie in [0, 56] and keep in [0, max_space / 2]";
+        return RISQGPU_ERR_INVALID;
+    }
+    h->dav_space = max_space;
+    h->dav_keep = keep;
+    return RISQGPU_OK;
+}
+
+int risqgpu_set_memory_limit(risqgpu_t* h, size_t bytes) {
+    if (!h) return RISQGPU_ERR_INVALID;
+    h->mem_limit = bytes;
+    return RISQGPU_OK;
+}
+
+int risqgpu_memory_used(const risqgpu_t* h, size_t* used, size_t* limit) {
+    if (!h) return RISQGPU_ERR_INVALID;
+    if (used) *used = h->mem_used;
+    if (limit) *limit = h->mem_limit;
     return RISQGPU_OK;
 }
 

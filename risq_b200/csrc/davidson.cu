@@ -76,8 +76,9 @@ struct SigmaTimer {
     }
 };
 
-constexpr int KMAX = 24;   // basis columns (nroots <= 8 -> at most 18)
+constexpr int KMAX = 64;   // basis columns (search space + the nroots new vectors)
 constexpr int RMAX = 8;    // roots
+constexpr int CCH = 16;    // basis columns per block of the dot-product kernels (blockIdx.y)
 constexpr int DBLK = 256;  // threads per reduction block
 
 __device__ __forceinline__ double warp_sum_d(double v) {
@@ -122,51 +123,73 @@ __global__ void k_reduce(const double* __restrict__ partial, int nblk, int m, in
     if (threadIdx.x == 0) out[j] = sh[0];
 }
 
-// dots[j] = <A_j, b> for j < m (A column-major, leading dimension N)
+// Partial dot products <A_j, b> (A column-major, leading dimension N) for the columns
+// j < m, and with `self` also <b, b> as column m; blockIdx.y takes CCH columns each.
+// partial[blockIdx.x * (KMAX + 1) + j].
 template <typename T>
-__global__ void __launch_bounds__(DBLK) k_multidot(const T* __restrict__ A, int m, const T* __restrict__ b, int64_t N,
-                                                  double* __restrict__ partial) {
-    double acc[KMAX];
+__global__ void __launch_bounds__(DBLK) k_dots(const T* __restrict__ A, int m, const T* __restrict__ b, int self,
+                                              int64_t N, double* __restrict__ partial) {
+    const int j0 = blockIdx.y * CCH;
+    const int mc = min(CCH, m + self - j0);
+    double acc[CCH];
 #pragma unroll
-    for (int j = 0; j < KMAX; j++) acc[j] = 0.0;
+    for (int j = 0; j < CCH; j++) acc[j] = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
-        double bi = (double)b[i];
+        const double bi = (double)b[i];
 #pragma unroll
-        for (int j = 0; j < KMAX; j++)
-            if (j < m) acc[j] += (double)A[j * N + i] * bi;
+        for (int j = 0; j < CCH; j++)
+            if (j < mc) acc[j] += (j0 + j < m ? (double)A[(int64_t)(j0 + j) * N + i] : bi) * bi;
     }
-    block_reduce_store<KMAX>(acc, m, partial, KMAX + 1);
+    block_reduce_store<CCH>(acc, mc, partial + j0, KMAX + 1);
 }
 
-// t -= sum_j coef[j] A_j ; then partial dots <A_j, t> (j < m) and <t, t> at slot m.
+// t -= sum_{j < m} coef[j] A_j, rounded to the basis type.
 template <typename T>
-__global__ void __launch_bounds__(DBLK) k_cgs(const T* __restrict__ A, int m, T* __restrict__ t, int64_t N,
-                                             const double* __restrict__ coef, double* __restrict__ partial) {
+__global__ void __launch_bounds__(DBLK) k_cgs_update(const T* __restrict__ A, int m, T* __restrict__ t, int64_t N,
+                                                    const double* __restrict__ coef) {
     __shared__ double c[KMAX];
     if (threadIdx.x < KMAX) c[threadIdx.x] = threadIdx.x < m ? coef[threadIdx.x] : 0.0;
     __syncthreads();
-    double acc[KMAX + 1];
-#pragma unroll
-    for (int j = 0; j <= KMAX; j++) acc[j] = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
-        double a[KMAX];
         double ti = (double)t[i];
-#pragma unroll
-        for (int j = 0; j < KMAX; j++)
-            if (j < m) { a[j] = (double)A[j * N + i]; ti -= c[j] * a[j]; }
-        T tt = (T)ti;
-        t[i] = tt;
-        ti = (double)tt;
-#pragma unroll
-        for (int j = 0; j < KMAX; j++)
-            if (j < m) acc[j] += a[j] * ti;
-        acc[KMAX] += ti * ti;
+        for (int j = 0; j < m; j++) ti -= c[j] * (double)A[(int64_t)j * N + i];
+        t[i] = (T)ti;
     }
-    // move the norm into slot m for the reduction
-    double out[KMAX + 1];
+}
+
+// Thick restart: out_V[:, c] = sum_j V[:, j] Y[j, c], out_HV likewise, for the columns
+// c of this block's chunk (blockIdx.y, CCH columns); Y: dim x keep, row-major.
+template <typename T>
+__global__ void __launch_bounds__(DBLK) k_combine(const T* __restrict__ V, const T* __restrict__ HV, int dim, int keep,
+                                                 int64_t N, const double* __restrict__ Y, T* __restrict__ outV,
+                                                 T* __restrict__ outHV) {
+    __shared__ double ys[KMAX * CCH];
+    const int c0 = blockIdx.y * CCH;
+    const int kc = min(CCH, keep - c0);
+    for (int k = threadIdx.x; k < dim * CCH; k += blockDim.x) {
+        const int j = k / CCH, c = k % CCH;
+        ys[k] = c < kc ? Y[j * keep + c0 + c] : 0.0;
+    }
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        double a[CCH], b[CCH];
 #pragma unroll
-    for (int j = 0; j <= KMAX; j++) out[j] = j < m ? acc[j] : (j == m ? acc[KMAX] : 0.0);
-    block_reduce_store<KMAX + 1>(out, m + 1, partial, KMAX + 1);
+        for (int c = 0; c < CCH; c++) { a[c] = 0.0; b[c] = 0.0; }
+        for (int j = 0; j < dim; j++) {
+            const double v = (double)V[(int64_t)j * N + i], hv = (double)HV[(int64_t)j * N + i];
+#pragma unroll
+            for (int c = 0; c < CCH; c++) {
+                a[c] += v * ys[j * CCH + c];
+                b[c] += hv * ys[j * CCH + c];
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CCH; c++)
+            if (c < kc) {
+                outV[(int64_t)(c0 + c) * N + i] = (T)a[c];
+                outHV[(int64_t)(c0 + c) * N + i] = (T)b[c];
+            }
+    }
 }
 
 template <typename T>
@@ -314,6 +337,15 @@ struct Work {
     double* coef = nullptr;     // KMAX+1
     double* cols = nullptr;     // (RMAX + KMAX) x (KMAX+1): reduced projected columns, then saved norms
     SigmaTimer timer;
+    // partial dots of the columns j < m of A with b (and <b, b> as column m when self)
+    template <typename T>
+    int dots(const T* A, int m, const T* b, bool self) {
+        const int cols = m + (self ? 1 : 0);
+        if (cols <= 0) return RISQGPU_OK;
+        dim3 g2(grid, (cols + CCH - 1) / CCH);
+        k_dots<T><<<g2, DBLK, 0, h->stream>>>(A, m, b, self ? 1 : 0, N, partial);
+        return check_launch(h, "dots");
+    }
     int reduce_to(int m, double* dev_out) {
         k_reduce<<<m, DBLK, 0, h->stream>>>(partial, grid, m, KMAX + 1, dev_out);
         return check_launch(h, "reduce");
@@ -338,17 +370,27 @@ struct LoopOut {
 
 // One Davidson run with basis type T.  init_int: internal-order FP64 columns (ninit)
 // or null for identity columns.  On return ritz (N x nr, FP64, internal order) holds
-// the last Ritz vectors.
+// the last Ritz vectors.  space: largest basis before a restart (the reference's
+// nroots + 10); keep: vectors kept at a restart (the reference keeps the nroots Ritz
+// vectors; more gives a thick restart with the lowest `keep` Ritz vectors).
 template <typename T>
 int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool normalize_init, const double* last_init,
                   double tol, double etol, int max_iter, int sigma_kind, float* fscale, double* ritz, double* hr,
-                  LoopOut& out) {
+                  int space, int keep, LoopOut& out) {
     risqgpu* h = wk.h;
     const int64_t N = wk.N;
-    const int mss = (int64_t)(nr + 10) < N ? nr + 10 : (int)N;
+    const int mss = (int64_t)space < N ? space : (int)N;
+    keep = std::max(nr, std::min(keep, mss - nr));
+    const bool thick = keep > nr;
     T *V = nullptr, *HV = nullptr;
-    RQ_TRY(dalloc(h, V, (size_t)(mss + nr) * N));
-    RQ_TRY(dalloc(h, HV, (size_t)(mss + nr) * N));
+    double* ybuf = nullptr;
+    ScopedFree<3> release(V, HV, ybuf);
+    // columns: the basis (mss), the new vectors (nr), and for a thick restart room for
+    // the kept combinations before they move to the front
+    const size_t ncols = (size_t)(mss + nr) + (thick ? (size_t)keep : 0);
+    RQ_TRY(dalloc(h, V, ncols * N));
+    RQ_TRY(dalloc(h, HV, ncols * N));
+    if (thick) RQ_TRY(dalloc(h, ybuf, (size_t)KMAX * KMAX));
     const int g = wk.grid;
     // initial subspace (generate_subspace, davidson.rs:318-338)
     int dim = init_int ? ninit : std::min(2, mss);
@@ -358,27 +400,33 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
         k_fill_init<T><<<g, DBLK, 0, h->stream>>>(V, dim, N, init_int, h->d_inv, 0, e1);
         RQ_TRY(check_launch(h, "init"));
     }
+    // Gram-Schmidt of column `col` of V against the columns before it, twice (classical
+    // Gram-Schmidt applied twice matches MGS to rounding); leaves |t|^2 in wk.red[col]
+    auto orthogonalise = [&](int col) -> int {
+        T* t = V + (size_t)col * N;
+        if (col > 0) {
+            RQ_TRY(wk.dots(V, col, t, false));
+            RQ_TRY(wk.reduce(col, nullptr));
+            for (int pass = 0; pass < 2; pass++) {
+                RQ_CUDA(h, cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * col, cudaMemcpyDeviceToDevice, h->stream));
+                k_cgs_update<T><<<g, DBLK, 0, h->stream>>>(V, col, t, N, wk.coef);
+                RQ_TRY(check_launch(h, "gram-schmidt"));
+                RQ_TRY(wk.dots(V, col, t, true));
+                RQ_TRY(wk.reduce(col + 1, nullptr));
+            }
+        } else {
+            RQ_TRY(wk.dots(V, 0, t, true));
+            RQ_TRY(wk.reduce(1, nullptr));
+        }
+        return RISQGPU_OK;
+    };
     // orthonormalise multi-column initial guesses; a single caller guess is used as given, as
     // in the reference, but a guess carried over from the FP32 stage is renormalised in FP64
     // (an FP32-rounded norm error of 1e-7 would shift the Rayleigh quotient by 1e-7 |E|)
     if (init_int && (dim > 1 || normalize_init)) {
         for (int c = 0; c < dim; c++) {
-            T* t = V + (size_t)c * N;
-            if (c > 0) {
-                k_multidot<T><<<g, DBLK, 0, h->stream>>>(V, c, t, N, wk.partial);
-                RQ_TRY(wk.reduce(c, nullptr));
-                cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * c, cudaMemcpyDeviceToDevice, h->stream);
-                k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, c, t, N, wk.coef, wk.partial);
-                RQ_TRY(wk.reduce(c + 1, nullptr));
-                cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * (c + 1), cudaMemcpyDeviceToDevice, h->stream);
-                k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, c, t, N, wk.coef, wk.partial);
-                RQ_TRY(wk.reduce(c + 1, nullptr));
-                k_scale<T><<<g, DBLK, 0, h->stream>>>(t, N, wk.red + c);
-            } else {
-                k_multidot<T><<<g, DBLK, 0, h->stream>>>(t, 1, t, N, wk.partial);
-                RQ_TRY(wk.reduce(1, nullptr));
-                k_scale<T><<<g, DBLK, 0, h->stream>>>(t, N, wk.red);
-            }
+            RQ_TRY(orthogonalise(c));
+            k_scale<T><<<g, DBLK, 0, h->stream>>>(V + (size_t)c * N, N, wk.red + c);
         }
     }
     for (int c = 0; c < dim; c++) RQ_TRY(wk.timer.run(h, V + (size_t)c * N, HV + (size_t)c * N, sigma_kind));
@@ -391,7 +439,7 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
     auto proj_cols = [&](int c0, int c1, int m, int extra) -> int {
         const int nc = c1 - c0;
         for (int c = c0; c < c1; c++) {
-            k_multidot<T><<<g, DBLK, 0, h->stream>>>(V, m, HV + (size_t)c * N, N, wk.partial);
+            RQ_TRY(wk.dots(V, m, HV + (size_t)c * N, false));
             RQ_TRY(wk.reduce_to(m, wk.cols + (size_t)(c - c0) * (KMAX + 1)));
         }
         const int nread = extra >= 0 ? extra + 1 : nc * (KMAX + 1);
@@ -410,7 +458,7 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
     RQ_TRY(proj_cols(0, dim, dim, -1));
     std::vector<double> last(nr, 0.0);
     if (last_init) for (int c = 0; c < nr; c++) last[c] = last_init[c];
-    std::vector<double> w(KMAX), Y(KMAX * KMAX), Pd(KMAX * KMAX), hostsmall(KMAX * RMAX + RMAX);
+    std::vector<double> w(KMAX), Y(KMAX * KMAX), Pd(KMAX * KMAX), hostsmall(KMAX * RMAX + RMAX), ykeep(KMAX * KMAX);
     std::vector<double> red(KMAX + 1);
     double e_feat = NAN;
     std::vector<double> res_hist;
@@ -472,19 +520,11 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
             const int norm_slot = nr * (KMAX + 1);
             for (int c = 0; c < nr; c++) {
                 const int col = dim + c;
-                T* t = V + (size_t)col * N;
-                k_multidot<T><<<g, DBLK, 0, h->stream>>>(V, col, t, N, wk.partial);
-                RQ_TRY(wk.reduce(col, nullptr));
-                RQ_CUDA(h, cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * col, cudaMemcpyDeviceToDevice, h->stream));
-                k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, col, t, N, wk.coef, wk.partial);
-                RQ_TRY(wk.reduce(col + 1, nullptr));
-                RQ_CUDA(h, cudaMemcpyAsync(wk.coef, wk.red, sizeof(double) * col, cudaMemcpyDeviceToDevice, h->stream));
-                k_cgs<T><<<g, DBLK, 0, h->stream>>>(V, col, t, N, wk.coef, wk.partial);
-                RQ_TRY(wk.reduce(col + 1, nullptr));
+                RQ_TRY(orthogonalise(col));
                 if (c == nr - 1)
                     RQ_CUDA(h, cudaMemcpyAsync(wk.cols + norm_slot, wk.red + col, sizeof(double),
                                                cudaMemcpyDeviceToDevice, h->stream));
-                k_scale<T><<<g, DBLK, 0, h->stream>>>(t, N, wk.red + col);
+                k_scale<T><<<g, DBLK, 0, h->stream>>>(V + (size_t)col * N, N, wk.red + col);
             }
             for (int c = 0; c < nr; c++)
                 RQ_TRY(wk.timer.run(h, V + (size_t)(dim + c) * N, HV + (size_t)(dim + c) * N, sigma_kind));
@@ -495,20 +535,34 @@ int davidson_loop(Work& wk, int nr, const double* init_int, int ninit, bool norm
             if (std::sqrt(saved_norm2) < 1e-9) { out.converged = true; out.reason = 2; break; }
             out.n_sigma += nr;
             dim += nr;
-        } else {
-            // restart to the Ritz vectors
+        } else if (!thick) {
+            // restart to the Ritz vectors (davidson.rs:261-269)
             k_set_cols<T><<<g, DBLK, 0, h->stream>>>(V, HV, ritz, hr, nr, N);
             RQ_TRY(check_launch(h, "restart"));
             dim = nr;
             std::fill(P.begin(), P.end(), 0.0);
             RQ_TRY(proj_cols(0, dim, dim, -1));
+        } else {
+            // thick restart: the lowest `keep` Ritz vectors and their H products, formed
+            // from the basis in the spare columns, then moved to the front
+            for (int j = 0; j < dim; j++)
+                for (int c = 0; c < keep; c++) ykeep[j * keep + c] = Y[j * dim + c];
+            RQ_CUDA(h, cudaMemcpyAsync(ybuf, ykeep.data(), sizeof(double) * dim * keep, cudaMemcpyHostToDevice,
+                                       h->stream));
+            T* sv = V + (size_t)(mss + nr) * N;
+            T* shv = HV + (size_t)(mss + nr) * N;
+            dim3 g2(g, (keep + CCH - 1) / CCH);
+            k_combine<T><<<g2, DBLK, 0, h->stream>>>(V, HV, dim, keep, N, ybuf, sv, shv);
+            RQ_TRY(check_launch(h, "thick restart"));
+            RQ_CUDA(h, cudaMemcpyAsync(V, sv, sizeof(T) * keep * N, cudaMemcpyDeviceToDevice, h->stream));
+            RQ_CUDA(h, cudaMemcpyAsync(HV, shv, sizeof(T) * keep * N, cudaMemcpyDeviceToDevice, h->stream));
+            dim = keep;
+            std::fill(P.begin(), P.end(), 0.0);
+            RQ_TRY(proj_cols(0, dim, dim, -1));
         }
     }
     out.iters += it + (it < max_iter ? 1 : 0);
-    RQ_TRY(sync(h, "davidson"));
-    dfree(V);
-    dfree(HV);
-    return RISQGPU_OK;
+    return sync(h, "davidson");
 }
 
 }  // namespace
@@ -520,7 +574,15 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
     if (!h->built) { h->err = "davidson before build"; return RISQGPU_ERR_INVALID; }
     if (nroots < 1 || nroots > RMAX) { h->err = "nroots must be in [1, 8]"; return RISQGPU_ERR_INVALID; }
     if ((size_t)nroots > h->N) { h->err = "nroots > N"; return RISQGPU_ERR_INVALID; }
-    if (init && (ninit < 1 || ninit > nroots + 10)) { h->err = "bad ninit"; return RISQGPU_ERR_INVALID; }
+    // search space and restart size: the reference's (nroots + 10, nroots) unless the
+    // handle was given others (risqgpu_set_subspace)
+    const int space = h->dav_space > 0 ? h->dav_space : nroots + 10;
+    const int keep = h->dav_keep > 0 ? h->dav_keep : nroots;
+    if (space + nroots > KMAX || space < 2 * nroots) {
+        h->err = "search space must lie in [2 nroots, " + std::to_string(KMAX) + " - nroots]";
+        return RISQGPU_ERR_INVALID;
+    }
+    if (init && (ninit < 1 || ninit > space)) { h->err = "bad ninit"; return RISQGPU_ERR_INVALID; }
     if (init && nroots > 1 && ninit < nroots) { h->err = "ninit must be >= nroots for several roots"; return RISQGPU_ERR_INVALID; }
     if (mode != RISQGPU_MODE_FP64 && (h->precision == RISQGPU_FP64 || h->precision == RISQGPU_COLS)) {
         h->err = "the FP32 sigma of MIXED / FP32 mode needs an FP32 or MIXED build";
@@ -535,19 +597,30 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         return RISQGPU_ERR_INVALID;
     }
     const int64_t N = (int64_t)h->N;
+    if (init) {
+        const size_t n_in = (size_t)ninit * h->N;
+        for (size_t i = 0; i < n_in; i++)
+            if (!std::isfinite(init[i])) {
+                h->err = "initial guess holds a non-finite value at index " + std::to_string(i);
+                return RISQGPU_ERR_INVALID;
+            }
+    }
     Work wk;
     wk.h = h;
     wk.N = N;
+    double *ritz = nullptr, *hr = nullptr, *init_int = nullptr, *tmp = nullptr, *seed = nullptr, *outv = nullptr;
+    float* fscale = nullptr;
+    ScopedFree<5> release_work(wk.partial, wk.red, wk.small, wk.coef, wk.cols);
+    ScopedFree<7> release_vecs(ritz, hr, init_int, tmp, seed, outv, fscale);
     wk.grid = std::max(1, std::min<int>((int)((N + DBLK - 1) / DBLK), num_sms(h) * 4));
     RQ_TRY(dalloc(h, wk.partial, (size_t)wk.grid * (KMAX + 1)));
     RQ_TRY(dalloc(h, wk.red, KMAX + 1));
     RQ_TRY(dalloc(h, wk.small, KMAX * RMAX + RMAX));
     RQ_TRY(dalloc(h, wk.coef, KMAX + 1));
     RQ_TRY(dalloc(h, wk.cols, (size_t)(KMAX + 2) * (KMAX + 1)));
-    double *ritz = nullptr, *hr = nullptr, *init_int = nullptr, *tmp = nullptr;
     RQ_TRY(dalloc(h, ritz, (size_t)nroots * N));
     RQ_TRY(dalloc(h, hr, (size_t)nroots * N));
-    int use_init = init ? std::min(ninit, nroots + 10) : 0;
+    int use_init = init ? std::min(ninit, space) : 0;
     if (init) {
         RQ_TRY(dalloc(h, tmp, (size_t)use_init * N));
         RQ_TRY(dalloc(h, init_int, (size_t)use_init * N));
@@ -555,29 +628,27 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         k_to_internal<<<wk.grid, DBLK, 0, h->stream>>>(tmp, h->d_orig, N, use_init, init_int);
         RQ_TRY(check_launch(h, "init"));
     }
-    float* fscale = nullptr;
     LoopOut lo;
     int n64 = 0;
     if (mode == RISQGPU_MODE_FP64) {
         if (precond == RISQGPU_PRECOND_LEARNED) RQ_TRY(dalloc(h, fscale, N));
         RQ_TRY(davidson_loop<double>(wk, nroots, init_int, use_init, false, nullptr, tol, etol, max_iter, 0, fscale, ritz, hr,
-                                     lo));
+                                     space, keep, lo));
         n64 = lo.n_sigma;
     } else {
         if (precond == RISQGPU_PRECOND_LEARNED) RQ_TRY(dalloc(h, fscale, N));
         RQ_TRY(davidson_loop<float>(wk, nroots, init_int, use_init, false, nullptr, tol, etol, max_iter, 1, fscale, ritz, hr,
-                                    lo));
+                                    space, keep, lo));
         const int n32 = lo.n_sigma;
         // closing FP64-sigma sweeps (stored FP32 + remainder, or elements recomputed in FP64);
         // FP32 mode stops after the FP32 stage
         if (lo.converged && mode == RISQGPU_MODE_MIXED) {
             // closing FP64-sigma sweeps from the FP64 Ritz vectors
             LoopOut lr;
-            double *seed = nullptr;
             RQ_TRY(dalloc(h, seed, (size_t)nroots * N));
             RQ_CUDA(h, cudaMemcpyAsync(seed, ritz, sizeof(double) * nroots * N, cudaMemcpyDeviceToDevice, h->stream));
             RQ_TRY(davidson_loop<double>(wk, nroots, seed, nroots, true, lo.evals, tol, etol, max_iter, 0, nullptr, ritz, hr,
-                                         lr));
+                                         space, keep, lr));
             dfree(seed);
             lr.iters += lo.iters;
             lr.fallbacks = lo.fallbacks;
@@ -588,17 +659,13 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
     }
     for (int c = 0; c < nroots; c++) evals[c] = lo.evals[c];
     if (evecs) {
-        double* outv = nullptr;
         RQ_TRY(dalloc(h, outv, (size_t)nroots * N));
         k_to_caller<<<wk.grid, DBLK, 0, h->stream>>>(ritz, h->d_orig, N, nroots, outv);
         RQ_CUDA(h, cudaMemcpyAsync(evecs, outv, sizeof(double) * nroots * N, cudaMemcpyDeviceToHost, h->stream));
         RQ_TRY(sync(h, "evecs"));
-        dfree(outv);
     }
     RQ_TRY(sync(h, "davidson end"));
     wk.timer.collect(h);
-    dfree(wk.partial); dfree(wk.red); dfree(wk.small); dfree(wk.coef); dfree(wk.cols);
-    dfree(ritz); dfree(hr); dfree(init_int); dfree(tmp); dfree(fscale);
     if (st) {
         st->iters = lo.iters;
         st->n_sigma = lo.n_sigma;

@@ -2,9 +2,11 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/risqgpu.h"
@@ -45,6 +47,10 @@ struct risqgpu {
     double sigma_ms_acc = 0.0;            // event time of sigma launches inside Davidson
     bool time_sigma = false;
     std::string err;
+    // device memory held by this handle through dalloc, and the caller's bound on it
+    // (0 = none; risqgpu_set_memory_limit)
+    size_t mem_used = 0;
+    size_t mem_limit = 0;
 
     // integrals (reference packed layout)
     int norb = 0;
@@ -100,6 +106,30 @@ struct risqgpu {
     uint64_t nnz_full = 0;
     uint64_t nnz_upper = 0;
 
+    // Tiled upper-triangle storage (upper builds).  Rows are cut into panels of
+    // 2^tile_rb consecutive rows and columns into windows of 2^tile_cb.  Each panel
+    // holds its dense (panel, window) tiles, elements coded (row in panel << tile_cb |
+    // column in window), followed by its leftover elements (pairs in tiles too sparse
+    // to stage), coded by their column, in row order.  Values share d_val64 / d_val32
+    // / d_val_lo with the element index.
+    bool tiled = false;
+    int tile_rb = 0, tile_cb = 0;
+    int64_t n_panels = 0;
+    int64_t n_tiles = 0;
+    uint64_t n_dense_el = 0;          // stored pairs in dense tiles
+    int64_t* d_panel_tile = nullptr;  // n_panels + 1: first tile of each panel
+    int32_t* d_tile_win = nullptr;    // window of each tile
+    int32_t* d_tile_len = nullptr;    // elements of each tile
+    int64_t* d_tile_off = nullptr;    // first element of each tile
+    int64_t* d_left_off = nullptr;    // N: first leftover element of each row
+    int32_t* d_left_len = nullptr;    // N: leftover elements of each row
+    uint32_t* d_el_idx = nullptr;     // element index (coded as above)
+    double h_row_abs_max = 0.0;       // max over rows of sum_q |H_pq| (both triangles), for the fixed-point scale
+    // sigma work space, allocated with the matrix: int64 fixed-point accumulators
+    // (N) and two scalars (max |x|, scale)
+    long long* d_acc = nullptr;
+    double* d_sig_scalars = nullptr;
+
     // previous build kept for an incremental extension
     size_t prev_N = 0;
     int32_t* d_prev_orig = nullptr;
@@ -115,6 +145,9 @@ struct risqgpu {
     std::vector<uint64_t> h_dets;
 
     risq::MlpWeights mlp;
+    // Davidson search space and restart size (0 = the reference's nroots + 10 and nroots)
+    int dav_space = 0;
+    int dav_keep = 0;
 
     // variational wavefunction of the last risqgpu_variational run (caller order)
     std::vector<uint64_t> wf_dets;
@@ -128,10 +161,18 @@ struct risqgpu {
 
 namespace risq {
 
+// Allocation ledger: every allocation made through dalloc is recorded with its handle
+// and size, so that dfree can return the bytes to that handle's count (mem_used).
+void mem_record(risqgpu* h, void* p, size_t bytes);
+void mem_forget(void* p);
+
 // Free a device pointer (ignores null) and reset it.
 template <typename T>
 inline void dfree(T*& p) {
-    if (p) cudaFree(p);
+    if (p) {
+        mem_forget((void*)p);
+        cudaFree(p);
+    }
     p = nullptr;
 }
 
@@ -139,15 +180,49 @@ template <typename T>
 inline int dalloc(risqgpu* h, T*& p, size_t count) {
     dfree(p);
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void**)&p, count * sizeof(T));
+    const size_t bytes = count * sizeof(T);
+    if (h->mem_limit && h->mem_used + bytes > h->mem_limit) {
+        h->err = "allocation of " + std::to_string(bytes) + " bytes exceeds the handle's device memory limit (" +
+                 std::to_string(h->mem_used) + " of " + std::to_string(h->mem_limit) + " bytes in use)";
+        return RISQGPU_ERR_OOM;
+    }
+    cudaError_t e = cudaMalloc((void**)&p, bytes);
     if (e != cudaSuccess) {
         p = nullptr;
         cudaGetLastError();
-        h->err = "cudaMalloc(" + std::to_string(count * sizeof(T)) + " bytes): " + cudaGetErrorString(e);
+        h->err = "cudaMalloc(" + std::to_string(bytes) + " bytes): " + cudaGetErrorString(e);
         return e == cudaErrorMemoryAllocation ? RISQGPU_ERR_OOM : RISQGPU_ERR_CUDA;
     }
+    mem_record(h, (void*)p, bytes);
     return RISQGPU_OK;
 }
+
+// Device bytes a new allocation may take: free device memory, bounded by the handle's limit.
+inline size_t mem_available(risqgpu* h) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+        cudaGetLastError();
+        fr = 0;
+    }
+    if (h->mem_limit) fr = std::min(fr, h->mem_limit > h->mem_used ? h->mem_limit - h->mem_used : (size_t)0);
+    return fr;
+}
+
+// Frees the device pointers it was given when it goes out of scope, so that every
+// early return of a function releases its work buffers.
+template <int K>
+struct ScopedFree {
+    void** slots[K];
+    template <typename... T>
+    explicit ScopedFree(T*&... p) : slots{reinterpret_cast<void**>(&p)...} {
+        static_assert(sizeof...(T) == K, "ScopedFree<K> takes K pointers");
+    }
+    ~ScopedFree() {
+        for (void** s : slots) dfree(*s);
+    }
+    ScopedFree(const ScopedFree&) = delete;
+    ScopedFree& operator=(const ScopedFree&) = delete;
+};
 
 inline int check_launch(risqgpu* h, const char* what) {
     cudaError_t e = cudaGetLastError();
@@ -185,6 +260,36 @@ void free_dets(risqgpu* h);
 // FP64 vectors, 1 = FP32 values on FP32 vectors.
 int sigma_device(risqgpu* h, const void* x, void* y, int kind);
 int sigma_host(risqgpu* h, const double* x, double* y, int nvec);
+// One FP64 vector between the caller's determinant order and the internal (sorted)
+// order, on the handle's stream: xi[p] = x[orig[p]] / y[orig[p]] = yi[p].
+int permute_in(risqgpu* h, const double* x, double* xi);
+int permute_out(risqgpu* h, const double* yi, double* y);
+
+// tiled upper-triangle storage (tiles.cu)
+int tile_shape(int64_t N, int& rb, int& cb);
+int sigma_tiles(risqgpu* h, const void* x, void* y, int kind);
+int tiles_coo(risqgpu* h, int32_t* p, int32_t* q, double* v);
+int tiles_self_energy(risqgpu* h, double energy, double gmin, double* out);
+int tiles_rows(risqgpu* h, const uint32_t* mark, int64_t* out_r, int64_t* out_c, double* out_v,
+               unsigned long long* count, unsigned long long cap);
+int export_rows_impl(risqgpu* h, const int64_t* rows, size_t k, int64_t* out_r, int64_t* out_c, double* out_v,
+                     size_t cap, size_t* count);
+void free_tiles(risqgpu* h);
+// Converts the CSR rows of a build, chunk by chunk of whole panels, into the tiled
+// arrays (d_el_idx and the value arrays must already hold room for every element).
+struct TileBuilder {
+    risqgpu* h = nullptr;
+    float* row_abs = nullptr;       // N: sum_q |H_pq| over both triangles
+    unsigned int* absmax = nullptr;
+    size_t tile_cap = 0;
+    int64_t el_next = 0, tile_next = 0;
+    int begin(risqgpu* h, int64_t n_panels);
+    template <typename VIN>
+    int chunk(int64_t p_lo, int64_t p_hi, const int64_t* row_start, int64_t base, const int32_t* row_len,
+              const int32_t* cols, const VIN* vin, const float* vlo_in, VIN* vout, float* vlo_out);
+    int finish();
+    ~TileBuilder();
+};
 
 // davidson (davidson.cu)
 int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double tol, double etol, int max_iter,

@@ -203,6 +203,7 @@ int precond_factors_impl(risqgpu* h, double energy, float* out) {
     if (h->N == 0) { h->err = "no determinants set"; return RISQGPU_ERR_INVALID; }
     const int64_t n = (int64_t)h->N;
     float *fi = nullptr, *fc = nullptr;
+    ScopedFree<2> release(fi, fc);
     RQ_TRY(dalloc(h, fi, n));
     RQ_TRY(dalloc(h, fc, n));
     RQ_TRY(mlp_scale_impl(h, energy, fi));

@@ -24,9 +24,14 @@
 // of 128 contiguous bytes, consecutive along K (leading byte offset 128 B), 8-row
 // groups K/8 core matrices apart (stride byte offset).
 // Every mbarrier wait is bounded in time; on a timeout the CTA records an error,
-// stops, and still frees its TMEM.
+// stops, and still frees its TMEM.  The timeout path is exercised by a test-only
+// switch (environment variable RISQGPU_TEST_MMA_STALL=1): the first completion wait
+// then watches a barrier that nothing arrives on, with a 1 ms limit, and the call
+// must come back with an error status while the handle stays usable.
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 
 #include "internal.cuh"
 
@@ -39,6 +44,7 @@ constexpr int TC_DETS = 64;    // determinants per tile
 constexpr int TC_H = 128;      // hidden width = MMA N
 constexpr int TC_THREADS = 128;
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per MMA completion wait
+constexpr unsigned long long STALL_PROBE_NS = 1000000ull;  // 1 ms: the test-only stalled wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -87,8 +93,8 @@ __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::be
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// wait for completion of phase `parity` of the mbarrier, at most WAIT_NS
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+// wait for completion of phase `parity` of the mbarrier, at most limit_ns
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, unsigned long long limit_ns = WAIT_NS) {
     const unsigned long long t0 = global_ns();
     while (true) {
         uint32_t done;
@@ -100,7 +106,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
             : "r"(mbar), "r"(parity)
             : "memory");
         if (done) return true;
-        if (global_ns() - t0 > WAIT_NS) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 
@@ -159,9 +165,10 @@ __global__ void __launch_bounds__(TC_THREADS) k_mlp_scale_tc(
     int norb, int K1, const double* __restrict__ h1, double energy, const uint16_t* __restrict__ w1,
     const float* __restrict__ bias1, const uint16_t* __restrict__ w2, const float* __restrict__ bias2,
     const uint16_t* __restrict__ w3, const float* __restrict__ bias3, float4 fnorm, float* __restrict__ out,
-    int* __restrict__ err) {
+    int* __restrict__ err, int stall_probe) {
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t mbar;
+    __shared__ __align__(8) uint64_t never_bar;  // nothing arrives on it (stall probe)
     __shared__ uint32_t tmem_slot;
     const TcSmem L = TcSmem::make(K1, norb);
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -197,6 +204,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_mlp_scale_tc(
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&never_bar)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -269,7 +277,9 @@ __global__ void __launch_bounds__(TC_THREADS) k_mlp_scale_tc(
                 mma_bf16(tmem, smem_desc(a1 + ks * 256, 128, sbo), smem_desc(b1 + ks * 256, 128, sbo), ks > 0);
             mma_commit(mb);
         }
-        bool ok = mbar_wait(mb, phase);
+        // the stall probe waits on a barrier whose phase never completes, so the bounded
+        // wait runs out; the MMA issued above completes on `mb` and is awaited below
+        bool ok = stall_probe ? mbar_wait(smem_u32(&never_bar), 0, STALL_PROBE_NS) : mbar_wait(mb, phase);
         if (!__syncthreads_and(ok)) {
             if (tid == 0) atomicExch(err, 1);
             mbar_wait(mb, phase);  // let the MMA in flight finish (bounded) before TMEM is freed
@@ -348,7 +358,10 @@ int mlp_scale_tc(risqgpu* h, double energy, float* out) {
     const TcSmem L = TcSmem::make(K1, h->norb);
     const int64_t N = (int64_t)h->N;
     int* err = nullptr;
+    ScopedFree<1> release(err);
     RQ_TRY(dalloc(h, err, 1));
+    const char* probe_env = std::getenv("RISQGPU_TEST_MMA_STALL");
+    const int stall_probe = (probe_env && std::strcmp(probe_env, "1") == 0) ? 1 : 0;
     RQ_CUDA(h, cudaMemsetAsync(err, 0, sizeof(int), h->stream));
     auto kern = k_mlp_scale_tc<1>;  // 2n <= 128: one word per spin string
     RQ_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
@@ -359,12 +372,11 @@ int mlp_scale_tc(risqgpu* h, double energy, float* out) {
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(ntiles, (int64_t)num_sms(h) * occ));
     kern<<<grid, TC_THREADS, L.total, h->stream>>>(h->d_up, h->d_dn, h->d_diag, N, h->norb, K1, h->d_h1, energy,
                                                    h->mlp.w1, h->mlp.b1, h->mlp.w2, h->mlp.b2, h->mlp.w3, h->mlp.b3,
-                                                   h->mlp.fnorm, out, err);
+                                                   h->mlp.fnorm, out, err, stall_probe);
     RQ_TRY(check_launch(h, "mlp scale (tensor cores)"));
     int herr = 0;
     RQ_CUDA(h, cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     RQ_TRY(sync(h, "mlp scale (tensor cores)"));
-    dfree(err);
     if (herr) {
         h->err = "tensor-core MLP: an MMA completion wait timed out";
         return RISQGPU_ERR_CUDA;

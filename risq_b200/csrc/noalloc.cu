@@ -55,18 +55,6 @@ int scratch_address(risqgpu* h, double** out) {
     return RISQGPU_OK;
 }
 
-__global__ void k_to_internal(const double* __restrict__ x, const int32_t* __restrict__ orig, int64_t n,
-                              double* __restrict__ xi) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
-        xi[p] = x[orig[p]];
-}
-
-__global__ void k_to_caller(const double* __restrict__ yi, const int32_t* __restrict__ orig, int64_t n,
-                            double* __restrict__ y) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
-        y[orig[p]] = yi[p];
-}
-
 }  // namespace
 
 }  // namespace risq
@@ -87,21 +75,23 @@ extern "C" int risqgpu_sigma_noalloc(risqgpu_t* h, const double* x_dev, double* 
     }
     int prev = -1;
     cudaGetDevice(&prev);
-    if (prev != h->device) cudaSetDevice(h->device);
+    if (prev != h->device) {
+        const cudaError_t e = cudaSetDevice(h->device);
+        if (e != cudaSuccess) {
+            h->err = std::string("cudaSetDevice(") + std::to_string(h->device) + "): " + cudaGetErrorString(e);
+            return RISQGPU_ERR_CUDA;
+        }
+    }
     double* scratch = nullptr;
     int rc = scratch_address(h, &scratch);
     if (rc == RISQGPU_OK) {
-        // both halves are written in full before they are read, so nothing is cleared
+        // both halves are written in full before they are read, so nothing is cleared;
+        // x is copied into the first half before y is written, so x_dev may equal y_dev
         double* xi = scratch;
         double* yi = scratch + kNoAllocMaxDets;
-        const int g = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
-        k_to_internal<<<g, 256, 0, h->stream>>>(x_dev, h->d_orig, n, xi);
-        rc = check_launch(h, "sigma_noalloc permute in");
+        rc = permute_in(h, x_dev, xi);
         if (rc == RISQGPU_OK) rc = sigma_device(h, xi, yi, 0);
-        if (rc == RISQGPU_OK) {
-            k_to_caller<<<g, 256, 0, h->stream>>>(yi, h->d_orig, n, y_dev);
-            rc = check_launch(h, "sigma_noalloc permute out");
-        }
+        if (rc == RISQGPU_OK) rc = permute_out(h, yi, y_dev);
         if (rc == RISQGPU_OK) rc = sync(h, "sigma_noalloc");
     }
     if (prev >= 0 && prev != h->device) cudaSetDevice(prev);

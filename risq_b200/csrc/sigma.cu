@@ -1,10 +1,11 @@
-// sigma = H x over the stored matrix (both triangles, diagonal kept apart).
+// sigma = H x over full-row storage (both triangles, diagonal kept apart), and the
+// dispatch to the tiled upper-triangle kernels (tiles.cu).
 //
-// Replaces SparseMatUpperTri::matrix_vector_prod (src/var/sparse.rs:64-78),
-// whose symmetric scatter into y[j] would need atomics on a GPU; the full
-// (both-triangle) rows make every output a private warp reduction instead.
-// One warp per row; the column/value streams are read once with evict-first
-// loads so that the gathered vector x stays resident in L2.
+// Replaces SparseMatUpperTri::matrix_vector_prod (src/var/sparse.rs:64-78).  With
+// both triangles stored every output is a private warp reduction: one warp per row,
+// the column/value streams read once with evict-first loads so that the gathered
+// vector x stays resident in L2.  Upper-triangle storage (the reference's own layout,
+// half the bytes) goes through the tiled kernels.
 #include <algorithm>
 #include <type_traits>
 
@@ -143,63 +144,6 @@ int launch_otf(risqgpu* h, const double* x, double* y) {
     return check_launch(h, "sigma otf");
 }
 
-// Upper-triangle storage: y = diag * x first, then every stored pair (p, q > p)
-// adds v x_q to y_p (warp sum, one atomic per row) and v x_p to y_q (one atomic per
-// element; y stays in L2).  V: value type (double, float, or float + float
-// remainder when VLO); X: vector type.
-template <typename X>
-__global__ void k_diag_times(int64_t N, const double* __restrict__ diag, const X* __restrict__ x, X* __restrict__ y) {
-    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
-        y[p] = (X)(diag[p] * (double)x[p]);
-}
-
-template <typename V, typename X, bool VLO>
-__global__ void __launch_bounds__(256) k_spmv_upper(int64_t N, const int64_t* __restrict__ row_start,
-                                                    const int32_t* __restrict__ row_len,
-                                                    const int32_t* __restrict__ cols, const V* __restrict__ vals,
-                                                    const float* __restrict__ vlo, const X* __restrict__ x,
-                                                    X* __restrict__ y) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t p = warp; p < N; p += nwarps) {
-        const int64_t s = row_start[p];
-        const int len = row_len[p];
-        const X xp = x[p];
-        X acc = 0;
-        int k = lane;
-        // four independent element loads in flight per lane before the gathers and scatters
-        for (; k + 96 < len; k += 128) {
-            const int c0 = __ldcs(cols + s + k), c1 = __ldcs(cols + s + k + 32);
-            const int c2 = __ldcs(cols + s + k + 64), c3 = __ldcs(cols + s + k + 96);
-            X v0 = (X)__ldcs(vals + s + k), v1 = (X)__ldcs(vals + s + k + 32);
-            X v2 = (X)__ldcs(vals + s + k + 64), v3 = (X)__ldcs(vals + s + k + 96);
-            if constexpr (VLO) {
-                v0 += (X)__ldcs(vlo + s + k); v1 += (X)__ldcs(vlo + s + k + 32);
-                v2 += (X)__ldcs(vlo + s + k + 64); v3 += (X)__ldcs(vlo + s + k + 96);
-            }
-            const X x0 = __ldg(x + c0), x1 = __ldg(x + c1), x2 = __ldg(x + c2), x3 = __ldg(x + c3);
-            acc += v0 * x0;
-            acc += v1 * x1;
-            acc += v2 * x2;
-            acc += v3 * x3;
-            atomicAdd(y + c0, v0 * xp);
-            atomicAdd(y + c1, v1 * xp);
-            atomicAdd(y + c2, v2 * xp);
-            atomicAdd(y + c3, v3 * xp);
-        }
-        for (; k < len; k += 32) {
-            const int c = __ldcs(cols + s + k);
-            X v = (X)__ldcs(vals + s + k);
-            if constexpr (VLO) v += (X)__ldcs(vlo + s + k);
-            acc += v * __ldg(x + c);
-            atomicAdd(y + c, v * xp);
-        }
-        acc = warp_sum(acc);
-        if (lane == 0) atomicAdd(y + p, acc);
-    }
-}
-
 __global__ void k_permute_in(const double* __restrict__ x, const int32_t* __restrict__ orig, int64_t n,
                              double* __restrict__ xi) {
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
@@ -265,25 +209,7 @@ int sigma_device(risqgpu* h, const void* x, void* y, int kind) {
     if (!h->built) { h->err = "sigma before build"; return RISQGPU_ERR_INVALID; }
     const int64_t n = (int64_t)h->N;
     const int grid = spmv_grid(h);
-    if (h->upper) {
-        const int g1 = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 16));
-        if (kind == 0) {
-            if (h->precision == RISQGPU_FP32) { h->err = "FP64 sigma needs FP64 or FP32 + remainder values"; return RISQGPU_ERR_INVALID; }
-            k_diag_times<double><<<g1, 256, 0, h->stream>>>(n, h->d_diag, (const double*)x, (double*)y);
-            if (h->precision == RISQGPU_FP64)
-                k_spmv_upper<double, double, false><<<grid, 256, 0, h->stream>>>(
-                    n, h->d_row_start, h->d_row_len, h->d_cols, h->d_val64, nullptr, (const double*)x, (double*)y);
-            else
-                k_spmv_upper<float, double, true><<<grid, 256, 0, h->stream>>>(
-                    n, h->d_row_start, h->d_row_len, h->d_cols, h->d_val32, h->d_val_lo, (const double*)x, (double*)y);
-        } else {
-            if (h->precision == RISQGPU_FP64) { h->err = "FP32 sigma needs FP32 values"; return RISQGPU_ERR_INVALID; }
-            k_diag_times<float><<<g1, 256, 0, h->stream>>>(n, h->d_diag, (const float*)x, (float*)y);
-            k_spmv_upper<float, float, false><<<grid, 256, 0, h->stream>>>(
-                n, h->d_row_start, h->d_row_len, h->d_cols, h->d_val32, nullptr, (const float*)x, (float*)y);
-        }
-        return check_launch(h, "sigma upper");
-    }
+    if (h->upper) return sigma_tiles(h, x, y, kind);
     if (kind == 0) {
         const double* xd = (const double*)x;
         double* yd = (double*)y;
@@ -306,25 +232,37 @@ int sigma_device(risqgpu* h, const void* x, void* y, int kind) {
     return check_launch(h, "sigma");
 }
 
+int permute_in(risqgpu* h, const double* x, double* xi) {
+    const int64_t n = (int64_t)h->N;
+    const int g = std::max(1, (int)std::min<int64_t>((n + 255) / 256, 148 * 16));
+    k_permute_in<<<g, 256, 0, h->stream>>>(x, h->d_orig, n, xi);
+    return check_launch(h, "permute in");
+}
+
+int permute_out(risqgpu* h, const double* yi, double* y) {
+    const int64_t n = (int64_t)h->N;
+    const int g = std::max(1, (int)std::min<int64_t>((n + 255) / 256, 148 * 16));
+    k_permute_out<<<g, 256, 0, h->stream>>>(yi, h->d_orig, n, y);
+    return check_launch(h, "permute out");
+}
+
 int sigma_host(risqgpu* h, const double* x, double* y, int nvec) {
     if (!h->built) { h->err = "sigma before build"; return RISQGPU_ERR_INVALID; }
     if (nvec < 1) { h->err = "nvec < 1"; return RISQGPU_ERR_INVALID; }
     const int64_t n = (int64_t)h->N;
     double *dx = nullptr, *dxi = nullptr, *dyi = nullptr;
+    ScopedFree<3> release(dx, dxi, dyi);
     RQ_TRY(dalloc(h, dx, n));
     RQ_TRY(dalloc(h, dxi, n));
     RQ_TRY(dalloc(h, dyi, n));
-    int g = std::max(1, (int)std::min<int64_t>((n + 255) / 256, 148 * 16));
     for (int c = 0; c < nvec; c++) {
         RQ_CUDA(h, cudaMemcpyAsync(dx, x + (size_t)c * n, sizeof(double) * n, cudaMemcpyHostToDevice, h->stream));
-        k_permute_in<<<g, 256, 0, h->stream>>>(dx, h->d_orig, n, dxi);
+        RQ_TRY(permute_in(h, dx, dxi));
         RQ_TRY(sigma_device(h, dxi, dyi, 0));
-        k_permute_out<<<g, 256, 0, h->stream>>>(dyi, h->d_orig, n, dx);
+        RQ_TRY(permute_out(h, dyi, dx));
         RQ_CUDA(h, cudaMemcpyAsync(y + (size_t)c * n, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
     }
-    RQ_TRY(sync(h, "sigma_host"));
-    dfree(dx); dfree(dxi); dfree(dyi);
-    return RISQGPU_OK;
+    return sync(h, "sigma_host");
 }
 
 int self_energy_impl(risqgpu* h, double energy, double gmin, double* out) {
@@ -333,9 +271,16 @@ int self_energy_impl(risqgpu* h, double energy, double gmin, double* out) {
     if (!(gmin > 0.0)) { h->err = "gmin must be positive"; return RISQGPU_ERR_INVALID; }
     const int64_t n = (int64_t)h->N;
     double *si = nullptr, *sc = nullptr;
+    ScopedFree<2> release(si, sc);
     RQ_TRY(dalloc(h, si, n));
     RQ_TRY(dalloc(h, sc, n));
     RQ_CUDA(h, cudaMemsetAsync(si, 0, sizeof(double) * n, h->stream));
+    if (h->tiled) {
+        RQ_TRY(tiles_self_energy(h, energy, gmin, si));
+        RQ_TRY(permute_out(h, si, sc));
+        RQ_CUDA(h, cudaMemcpyAsync(out, sc, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+        return sync(h, "self energy");
+    }
     const int grid = spmv_grid(h);
     const int up = h->upper ? 1 : 0;
     if (h->precision == RISQGPU_FP64)
@@ -348,13 +293,9 @@ int self_energy_impl(risqgpu* h, double energy, double gmin, double* out) {
         k_self_energy<1><<<grid, 256, 0, h->stream>>>(n, h->d_row_start, h->d_row_len, h->d_cols, nullptr, h->d_val32,
                                                       nullptr, h->d_diag, energy, gmin, up, si);
     RQ_TRY(check_launch(h, "self energy"));
-    int g = std::max(1, (int)std::min<int64_t>((n + 255) / 256, 148 * 16));
-    k_permute_out<<<g, 256, 0, h->stream>>>(si, h->d_orig, n, sc);
+    RQ_TRY(permute_out(h, si, sc));
     RQ_CUDA(h, cudaMemcpyAsync(out, sc, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
-    RQ_TRY(sync(h, "self energy"));
-    dfree(si);
-    dfree(sc);
-    return RISQGPU_OK;
+    return sync(h, "self energy");
 }
 
 }  // namespace risq

@@ -1,0 +1,756 @@
+// Tiled upper-triangle storage and its sigma.
+//
+// The reference's SparseMatUpperTri (src/var/sparse.rs:24-36) holds every pair
+// once and its matrix_vector_prod (src/var/sparse.rs:64-78) adds each element to
+// two outputs: y_p += H_pq x_q and y_q += H_pq x_p.  On the GPU the second of
+// these is a scattered atomic per pair, and a gather plus a scattered atomic per
+// pair bound the plain kernel by L1/L2 request throughput, not by HBM.
+//
+// Here the stored pairs are regrouped after the build.  Rows are cut into panels
+// of R = 2^rb consecutive rows and columns into windows of C = 2^cb.  A (panel,
+// window) tile that holds enough pairs is "dense": sigma stages x of its window
+// and zeroes a window of accumulators in shared memory, so that every pair costs
+// two shared-memory updates and the global traffic per tile is one coalesced read
+// of x and one coalesced flush of the accumulated column sums.  Pairs of sparse
+// tiles stay as leftovers, kept in row order and summed per row by a warp with
+// global gathers and atomics, as in the plain kernel.  Within a panel the row sums
+// gather in a shared panel accumulator that is flushed once.
+//
+// Sums are formed in 64-bit fixed point: each product v x is rounded to an integer
+// multiple of 2^-s and added with integer atomics, which are associative, so the
+// result does not depend on the order in which the pairs land and two runs give
+// bitwise-equal vectors.  s is chosen per call from max |x| and the largest row
+// sum of |H| over both triangles (found during the conversion), so that no sum can
+// exceed 2^62; the rounding error of a sum of m products is below m 2^-(s+1).
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <type_traits>
+
+#include "internal.cuh"
+
+namespace risq {
+
+namespace {
+
+constexpr int TT = 256;          // threads per CTA of the conversion and sigma kernels
+constexpr int MAX_BINS = 16384;  // windows one panel may span during the conversion
+constexpr unsigned FULL = 0xffffffffu;
+
+// A tile is staged in shared memory when it holds at least max(DENSE_MIN, w >> DENSE_SHIFT)
+// pairs (w = width of its window): staging w values of x, zeroing w accumulators and
+// flushing them costs about as much as w >> DENSE_SHIFT scattered pairs.
+constexpr int DENSE_MIN = 64;
+constexpr int DENSE_SHIFT = 3;
+
+__host__ __device__ __forceinline__ bool dense_tile(int count, int w) {
+    return count >= DENSE_MIN && count >= (w >> DENSE_SHIFT);
+}
+
+__device__ __forceinline__ int window_width(int64_t N, int64_t J, int cb) {
+    const int64_t c0 = J << cb;
+    return (int)min((int64_t)1 << cb, N - c0);
+}
+
+// ---------------------------------------------------------------- conversion
+
+// Per panel of the chunk [p_lo, p_hi): stored pairs, pairs in dense tiles, dense
+// tiles, and per row the number of leftover pairs.  CSR input: row p's columns at
+// cols[row_start[p] - base ...], row_len[p] of them.
+__global__ void __launch_bounds__(TT) k_tile_count(int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb,
+                                                   const int64_t* __restrict__ row_start, int64_t base,
+                                                   const int32_t* __restrict__ row_len,
+                                                   const int32_t* __restrict__ cols, int64_t* __restrict__ panel_nel,
+                                                   int64_t* __restrict__ panel_dense_el,
+                                                   int32_t* __restrict__ panel_ntiles,
+                                                   int32_t* __restrict__ left_len) {
+    extern __shared__ int32_t hist[];
+    using BR = cub::BlockReduce<long long, TT>;
+    __shared__ typename BR::TempStorage red;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int64_t P = p_lo + blockIdx.x; P < p_hi; P += gridDim.x) {
+        const int64_t r0 = P << rb, r1 = min(N, r0 + ((int64_t)1 << rb));
+        const int64_t J0 = r0 >> cb;
+        const int nb = (int)(((N - 1) >> cb) - J0 + 1);
+        for (int b = threadIdx.x; b < nb; b += TT) hist[b] = 0;
+        __syncthreads();
+        long long my_nel = 0;
+        for (int64_t r = r0 + warp; r < r1; r += TT / 32) {
+            const int64_t s = row_start[r] - base;
+            const int len = row_len[r];
+            if (lane == 0) my_nel += len;
+            for (int k = lane; k < len; k += 32) atomicAdd(&hist[(cols[s + k] >> cb) - J0], 1);
+        }
+        __syncthreads();
+        long long my_tiles = 0, my_dense = 0;
+        for (int b = threadIdx.x; b < nb; b += TT) {
+            const int c = hist[b];
+            if (c > 0 && dense_tile(c, window_width(N, J0 + b, cb))) {
+                my_tiles++;
+                my_dense += c;
+            }
+        }
+        // leftover pairs of every row (pairs whose tile is not dense)
+        for (int64_t r = r0 + warp; r < r1; r += TT / 32) {
+            const int64_t s = row_start[r] - base;
+            const int len = row_len[r];
+            int nl = 0;
+            for (int k = lane; k < len; k += 32) {
+                const int64_t b = (cols[s + k] >> cb) - J0;
+                nl += dense_tile(hist[b], window_width(N, J0 + b, cb)) ? 0 : 1;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) nl += __shfl_xor_sync(FULL, nl, o);
+            if (lane == 0) left_len[r] = nl;
+        }
+        const long long t_nel = BR(red).Sum(my_nel);
+        __syncthreads();
+        const long long t_tiles = BR(red).Sum(my_tiles);
+        __syncthreads();
+        const long long t_dense = BR(red).Sum(my_dense);
+        if (threadIdx.x == 0) {
+            panel_nel[P - p_lo] = t_nel;
+            panel_ntiles[P - p_lo] = (int32_t)t_tiles;
+            panel_dense_el[P - p_lo] = t_dense;
+        }
+        __syncthreads();
+    }
+}
+
+// Scatter the chunk's pairs into the tiled arrays.  panel_el_off / panel_tile_off:
+// absolute first element / first tile of every panel of the chunk.  Also adds |H_pq|
+// to the row sums of both p and q (row_abs, for the fixed-point scale).
+template <typename VIN>
+__global__ void __launch_bounds__(TT) k_tile_scatter(
+    int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb, const int64_t* __restrict__ row_start, int64_t base,
+    const int32_t* __restrict__ row_len, const int32_t* __restrict__ cols, const VIN* __restrict__ vin,
+    const float* __restrict__ vlo_in, const int64_t* __restrict__ panel_el_off,
+    const int64_t* __restrict__ panel_tile_off, const int64_t* __restrict__ panel_dense_el,
+    const int32_t* __restrict__ left_len, int32_t* __restrict__ tile_win, int32_t* __restrict__ tile_len,
+    int64_t* __restrict__ tile_off, int64_t* __restrict__ left_off, uint32_t* __restrict__ el_idx,
+    VIN* __restrict__ vout, float* __restrict__ vlo_out, float* __restrict__ row_abs) {
+    extern __shared__ int32_t sm_i[];
+    int32_t* cursor = sm_i;              // per window: next dense slot (panel-relative), or -1
+    int32_t* lcur = sm_i + MAX_BINS;     // per row of the panel: leftover start (panel-relative)
+    using BS = cub::BlockScan<long long, TT>;
+    __shared__ typename BS::TempStorage scan;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const uint32_t cmask = (1u << cb) - 1u;
+    for (int64_t P = p_lo + blockIdx.x; P < p_hi; P += gridDim.x) {
+        const int64_t r0 = P << rb, r1 = min(N, r0 + ((int64_t)1 << rb));
+        const int nr = (int)(r1 - r0);
+        const int64_t J0 = r0 >> cb;
+        const int nb = (int)(((N - 1) >> cb) - J0 + 1);
+        const int64_t el0 = panel_el_off[P - p_lo];
+        const int64_t t0 = panel_tile_off[P - p_lo];
+        for (int b = threadIdx.x; b < nb; b += TT) cursor[b] = 0;
+        __syncthreads();
+        for (int64_t r = r0 + warp; r < r1; r += TT / 32) {
+            const int64_t s = row_start[r] - base;
+            const int len = row_len[r];
+            for (int k = lane; k < len; k += 32) atomicAdd(&cursor[(cols[s + k] >> cb) - J0], 1);
+        }
+        __syncthreads();
+        // dense windows in window order: element and tile prefix sums over contiguous
+        // chunks of windows per thread
+        const int per = (nb + TT - 1) / TT;
+        const int b_lo = min(nb, (int)threadIdx.x * per), b_hi = min(nb, b_lo + per);
+        long long my_el = 0, my_t = 0;
+        for (int b = b_lo; b < b_hi; b++) {
+            const int c = cursor[b];
+            if (c > 0 && dense_tile(c, window_width(N, J0 + b, cb))) {
+                my_el += c;
+                my_t++;
+            }
+        }
+        long long ex_el, ex_t;
+        BS(scan).ExclusiveSum(my_el, ex_el);
+        __syncthreads();
+        BS(scan).ExclusiveSum(my_t, ex_t);
+        __syncthreads();
+        for (int b = b_lo; b < b_hi; b++) {
+            const int c = cursor[b];
+            if (c > 0 && dense_tile(c, window_width(N, J0 + b, cb))) {
+                tile_win[t0 + ex_t] = (int32_t)(J0 + b);
+                tile_len[t0 + ex_t] = c;
+                tile_off[t0 + ex_t] = el0 + ex_el;
+                cursor[b] = (int32_t)ex_el;
+                ex_el += c;
+                ex_t++;
+            } else {
+                cursor[b] = -1;
+            }
+        }
+        // leftover regions of the rows, in row order after the dense tiles
+        {
+            const int rper = (nr + TT - 1) / TT;
+            const int q_lo = min(nr, (int)threadIdx.x * rper), q_hi = min(nr, q_lo + rper);
+            long long my_l = 0;
+            for (int i = q_lo; i < q_hi; i++) my_l += left_len[r0 + i];
+            long long ex_l;
+            BS(scan).ExclusiveSum(my_l, ex_l);
+            const long long dense_total = panel_dense_el[P - p_lo];
+            for (int i = q_lo; i < q_hi; i++) {
+                lcur[i] = (int32_t)(dense_total + ex_l);
+                left_off[r0 + i] = el0 + dense_total + ex_l;
+                ex_l += left_len[r0 + i];
+            }
+        }
+        __syncthreads();
+        for (int64_t r = r0 + warp; r < r1; r += TT / 32) {
+            const int64_t s = row_start[r] - base;
+            const int len = row_len[r];
+            const uint32_t lr = (uint32_t)(r - r0);
+            int lnext = lcur[lr];
+            float rsum = 0.f;
+            for (int k0 = 0; k0 < len; k0 += 32) {
+                const int k = k0 + lane;
+                const bool act = k < len;
+                int q = 0;
+                int32_t cur = -1;
+                if (act) {
+                    q = cols[s + k];
+                    cur = cursor[(q >> cb) - J0];
+                }
+                const bool left = act && cur < 0;
+                const unsigned ml = __ballot_sync(FULL, left);
+                int64_t pos = 0;
+                uint32_t code = 0;
+                if (act) {
+                    if (left) {
+                        pos = el0 + lnext + __popc(ml & lt);
+                        code = (uint32_t)q;
+                    } else {
+                        pos = el0 + atomicAdd(&cursor[(q >> cb) - J0], 1);
+                        code = (lr << cb) | ((uint32_t)q & cmask);
+                    }
+                    el_idx[pos] = code;
+                    const VIN v = vin[s + k];
+                    vout[pos] = v;
+                    float av = fabsf((float)v);
+                    if (vlo_in) {
+                        vlo_out[pos] = vlo_in[s + k];
+                        av = (float)fabs((double)v + (double)vlo_in[s + k]);
+                    }
+                    rsum += av;
+                    atomicAdd(row_abs + q, av);
+                }
+                lnext += __popc(ml);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) rsum += __shfl_xor_sync(FULL, rsum, o);
+            if (lane == 0) atomicAdd(row_abs + r, rsum);
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_widen(const int32_t* __restrict__ a, int64_t n, int64_t* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = a[i];
+}
+
+__global__ void k_max_f32(const float* __restrict__ a, int64_t n, unsigned int* __restrict__ out) {
+    float m = 0.f;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, a[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // non-negative floats order as integers
+}
+
+// ---------------------------------------------------------------- sigma
+
+template <typename X>
+__global__ void k_absmax(const X* __restrict__ x, int64_t n, unsigned long long* __restrict__ out) {
+    double m = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmax(m, fabs((double)x[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(FULL, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+// scalars[0]: max |x| (bits), scalars[1] <- 2^s, scalars[2] <- 2^-s, scalars[3]: panel counter
+__global__ void k_fixed_scale(double* __restrict__ scalars, double row_abs_max, int smax) {
+    const double xmax = __longlong_as_double(*(const long long*)scalars);
+    const double bound = row_abs_max * xmax;
+    int s = 0;
+    if (bound > 0.0 && isfinite(bound)) s = 61 - ilogb(bound);
+    s = max(-smax, min(smax, s));
+    scalars[1] = ldexp(1.0, s);
+    scalars[2] = ldexp(1.0, -s);
+    reinterpret_cast<unsigned long long*>(scalars)[3] = 0ull;
+}
+
+template <typename X>
+__device__ __forceinline__ long long to_fixed(X t, X scale);
+template <>
+__device__ __forceinline__ long long to_fixed<float>(float t, float scale) {
+    return __float2ll_rn(t * scale);
+}
+template <>
+__device__ __forceinline__ long long to_fixed<double>(double t, double scale) {
+    return __double2ll_rn(t * scale);
+}
+
+__device__ __forceinline__ void sadd(long long* a, long long v) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(a), (unsigned long long)v);
+}
+
+// V: stored value type; VLO: add the FP32 remainder (MIXED storage); X: vector type.
+template <typename V, typename X, bool VLO>
+__global__ void __launch_bounds__(TT) k_sigma_tiles(
+    int64_t N, int64_t n_panels, int rb, int cb, const int64_t* __restrict__ panel_tile,
+    const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
+    const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len, const uint32_t* __restrict__ el_idx,
+    const V* __restrict__ vals, const float* __restrict__ vlo, const X* __restrict__ x,
+    long long* __restrict__ acc, double* __restrict__ scalars) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int R = 1 << rb, C = 1 << cb;
+    long long* yP = reinterpret_cast<long long*>(sm);
+    long long* yJ = yP + R;
+    X* xP = reinterpret_cast<X*>(yJ + C);
+    X* xJ = xP + R;
+    __shared__ long long s_panel;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t cmask = (uint32_t)C - 1u;
+    const X scale = (X)scalars[1];
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
+    for (;;) {
+        if (threadIdx.x == 0) s_panel = (long long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const int64_t P = s_panel;
+        if (P >= n_panels) break;
+        const int64_t r0 = P << rb;
+        const int nr = (int)min((int64_t)R, N - r0);
+        for (int i = threadIdx.x; i < nr; i += TT) {
+            xP[i] = x[r0 + i];
+            yP[i] = 0;
+        }
+        __syncthreads();
+        const int64_t tb = panel_tile[P], te = panel_tile[P + 1];
+        for (int64_t t = tb; t < te; t++) {
+            const int64_t c0 = (int64_t)tile_win[t] << cb;
+            const int w = (int)min((int64_t)C, N - c0);
+            const int64_t e0 = tile_off[t];
+            const int len = tile_len[t];
+            for (int i = threadIdx.x; i < w; i += TT) {
+                xJ[i] = x[c0 + i];
+                yJ[i] = 0;
+            }
+            __syncthreads();
+            int k = threadIdx.x;
+            for (; k + 3 * TT < len; k += 4 * TT) {
+                uint32_t u[4];
+                X v[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    u[j] = __ldcs(el_idx + e0 + k + j * TT);
+                    v[j] = (X)__ldcs(vals + e0 + k + j * TT);
+                    if constexpr (VLO) v[j] += (X)__ldcs(vlo + e0 + k + j * TT);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const uint32_t lr = u[j] >> cb, lc = u[j] & cmask;
+                    if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;  // never taken for a valid layout
+                    sadd(yP + lr, to_fixed<X>(v[j] * xJ[lc], scale));
+                    sadd(yJ + lc, to_fixed<X>(v[j] * xP[lr], scale));
+                }
+            }
+            for (; k < len; k += TT) {
+                const uint32_t u = __ldcs(el_idx + e0 + k);
+                X v = (X)__ldcs(vals + e0 + k);
+                if constexpr (VLO) v += (X)__ldcs(vlo + e0 + k);
+                const uint32_t lr = u >> cb, lc = u & cmask;
+                if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;
+                sadd(yP + lr, to_fixed<X>(v * xJ[lc], scale));
+                sadd(yJ + lc, to_fixed<X>(v * xP[lr], scale));
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < w; i += TT) {
+                const long long a = yJ[i];
+                if (a != 0) sadd(acc + c0 + i, a);
+            }
+            __syncthreads();
+        }
+        // leftover pairs: one warp per row, private row sum, column sums by global atomics
+        for (int i = warp; i < nr; i += TT / 32) {
+            const int64_t s = left_off[r0 + i];
+            const int len = left_len[r0 + i];
+            const X xr = xP[i];
+            X rs = 0;
+            int k = lane;
+            for (; k + 96 < len; k += 128) {
+                uint32_t q[4];
+                X v[4];
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    q[j] = __ldcs(el_idx + s + k + 32 * j);
+                    v[j] = (X)__ldcs(vals + s + k + 32 * j);
+                    if constexpr (VLO) v[j] += (X)__ldcs(vlo + s + k + 32 * j);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    if (q[j] >= (uint64_t)N) continue;  // never taken for a valid layout
+                    rs += v[j] * __ldg(x + q[j]);
+                    sadd(acc + q[j], to_fixed<X>(v[j] * xr, scale));
+                }
+            }
+            for (; k < len; k += 32) {
+                const uint32_t q = __ldcs(el_idx + s + k);
+                X v = (X)__ldcs(vals + s + k);
+                if constexpr (VLO) v += (X)__ldcs(vlo + s + k);
+                if (q >= (uint64_t)N) continue;
+                rs += v * __ldg(x + q);
+                sadd(acc + q, to_fixed<X>(v * xr, scale));
+            }
+            // fixed lane order: the warp sum does not depend on timing
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(FULL, rs, o);
+            if (lane == 0 && len > 0) sadd(yP + i, to_fixed<X>(rs, scale));
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nr; i += TT) {
+            const long long a = yP[i];
+            if (a != 0) sadd(acc + r0 + i, a);
+        }
+        __syncthreads();
+    }
+}
+
+// y = diag x + acc 2^-s
+template <typename X>
+__global__ void k_fixed_finish(int64_t N, const double* __restrict__ diag, const X* __restrict__ x,
+                               const long long* __restrict__ acc, const double* __restrict__ scalars,
+                               X* __restrict__ y) {
+    const double inv = scalars[2];
+    for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
+        y[p] = (X)(diag[p] * (double)x[p] + (double)acc[p] * inv);
+}
+
+// Calls f(p, q, v) for every stored pair (p < q, internal indices, FP64 value):
+// one CTA per panel, its dense tiles and then its leftover rows.
+template <typename V, bool VLO, typename F>
+__global__ void __launch_bounds__(TT) k_tiles_each(int64_t N, int64_t n_panels, int rb, int cb,
+                                                  const int64_t* __restrict__ panel_tile,
+                                                  const int32_t* __restrict__ tile_win,
+                                                  const int32_t* __restrict__ tile_len,
+                                                  const int64_t* __restrict__ tile_off,
+                                                  const int64_t* __restrict__ left_off,
+                                                  const int32_t* __restrict__ left_len,
+                                                  const uint32_t* __restrict__ el_idx, const V* __restrict__ vals,
+                                                  const float* __restrict__ vlo, F f) {
+    const uint32_t cmask = (1u << cb) - 1u;
+    for (int64_t P = blockIdx.x; P < n_panels; P += gridDim.x) {
+        const int64_t r0 = P << rb;
+        for (int64_t t = panel_tile[P]; t < panel_tile[P + 1]; t++) {
+            const int64_t c0 = (int64_t)tile_win[t] << cb, e0 = tile_off[t];
+            for (int k = threadIdx.x; k < tile_len[t]; k += TT) {
+                const uint32_t u = el_idx[e0 + k];
+                double v = (double)vals[e0 + k];
+                if constexpr (VLO) v += (double)vlo[e0 + k];
+                f(r0 + (u >> cb), c0 + (u & cmask), v, e0 + k);
+            }
+        }
+        const int nr = (int)min((int64_t)1 << rb, N - r0);
+        for (int i = 0; i < nr; i++) {
+            const int64_t s = left_off[r0 + i];
+            for (int k = threadIdx.x; k < left_len[r0 + i]; k += TT) {
+                double v = (double)vals[s + k];
+                if constexpr (VLO) v += (double)vlo[s + k];
+                f(r0 + i, (int64_t)el_idx[s + k], v, s + k);
+            }
+        }
+    }
+}
+
+struct CooOut {
+    int32_t* p;
+    int32_t* q;
+    double* v;
+    __device__ void operator()(int64_t pp, int64_t qq, double vv, int64_t e) const {
+        p[e] = (int32_t)pp;
+        q[e] = (int32_t)qq;
+        v[e] = vv;
+    }
+};
+
+struct SelfEnergyAdd {
+    const double* diag;
+    double energy, gmin;
+    double* out;
+    __device__ void operator()(int64_t pp, int64_t qq, double vv, int64_t) const {
+        const double v2 = vv * vv;
+        atomicAdd(out + pp, -v2 / fmax(diag[qq] - energy, gmin));
+        atomicAdd(out + qq, -v2 / fmax(diag[pp] - energy, gmin));
+    }
+};
+
+// Stored pairs that touch a marked row (bitmap over internal indices), in the caller's
+// indices, both orientations: (row, column, value) with the row marked.
+struct RowFilter {
+    const uint32_t* mark;
+    const int32_t* orig;
+    int64_t* out_r;
+    int64_t* out_c;
+    double* out_v;
+    unsigned long long* count;
+    unsigned long long cap;
+    __device__ void emit(int64_t r, int64_t c, double v) const {
+        const unsigned long long k = atomicAdd(count, 1ull);
+        if (k < cap) {
+            out_r[k] = orig[r];
+            out_c[k] = orig[c];
+            out_v[k] = v;
+        }
+    }
+    __device__ void operator()(int64_t pp, int64_t qq, double vv, int64_t) const {
+        if ((mark[pp >> 5] >> (pp & 31)) & 1u) emit(pp, qq, vv);
+        if ((mark[qq >> 5] >> (qq & 31)) & 1u) emit(qq, pp, vv);
+    }
+};
+
+template <typename F>
+int tiles_each(risqgpu* h, F f) {
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h->n_panels, (int64_t)num_sms(h) * 8));
+#define RQ_EACH(V, VLO, vals, lo)                                                                                   \
+    k_tiles_each<V, VLO, F><<<grid, TT, 0, h->stream>>>((int64_t)h->N, h->n_panels, h->tile_rb, h->tile_cb,         \
+                                                         h->d_panel_tile, h->d_tile_win, h->d_tile_len,             \
+                                                         h->d_tile_off, h->d_left_off, h->d_left_len, h->d_el_idx, \
+                                                         vals, lo, f)
+    if (h->precision == RISQGPU_FP64) RQ_EACH(double, false, h->d_val64, nullptr);
+    else if (h->precision == RISQGPU_MIXED) RQ_EACH(float, true, h->d_val32, h->d_val_lo);
+    else RQ_EACH(float, false, h->d_val32, nullptr);
+#undef RQ_EACH
+    return check_launch(h, "tiled pairs");
+}
+
+inline int grid_n(risqgpu* h, int64_t n) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms(h) * 16));
+}
+
+template <typename V, typename X, bool VLO>
+int launch_tiles(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo) {
+    const int64_t N = (int64_t)h->N;
+    const int R = 1 << h->tile_rb, C = 1 << h->tile_cb;
+    const size_t smem = (size_t)(R + C) * (sizeof(long long) + sizeof(X));
+    auto kern = k_sigma_tiles<V, X, VLO>;
+    static int attr_set[64] = {0};
+    const int dev = h->device & 63;
+    if (attr_set[dev] < (int)smem) {
+        RQ_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set[dev] = (int)smem;
+    }
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem);
+    const int grid = (int)std::min<int64_t>(h->n_panels, (int64_t)num_sms(h) * std::max(occ, 1));
+    RQ_CUDA(h, cudaMemsetAsync(h->d_acc, 0, sizeof(long long) * N, h->stream));
+    RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double), h->stream));
+    k_absmax<X><<<grid_n(h, N), 256, 0, h->stream>>>(x, N, reinterpret_cast<unsigned long long*>(h->d_sig_scalars));
+    k_fixed_scale<<<1, 1, 0, h->stream>>>(h->d_sig_scalars, h->h_row_abs_max, std::is_same<X, float>::value ? 100 : 1000);
+    kern<<<std::max(grid, 1), TT, smem, h->stream>>>(N, h->n_panels, h->tile_rb, h->tile_cb, h->d_panel_tile,
+                                                    h->d_tile_win, h->d_tile_len, h->d_tile_off, h->d_left_off,
+                                                    h->d_left_len, h->d_el_idx, vals, vlo, x, h->d_acc,
+                                                    h->d_sig_scalars);
+    k_fixed_finish<X><<<grid_n(h, N), 256, 0, h->stream>>>(N, h->d_diag, x, h->d_acc, h->d_sig_scalars, y);
+    return check_launch(h, "sigma (tiles)");
+}
+
+// Grow a device array to hold `need` entries, keeping the first `keep`.
+template <typename T>
+int grow(risqgpu* h, T*& p, size_t& capacity, size_t need, size_t keep) {
+    if (need <= capacity) return RISQGPU_OK;
+    size_t nc = std::max(need, capacity + capacity / 2);
+    T* q = nullptr;
+    RQ_TRY(dalloc(h, q, nc));
+    if (p && keep) RQ_CUDA(h, cudaMemcpyAsync(q, p, sizeof(T) * keep, cudaMemcpyDeviceToDevice, h->stream));
+    RQ_TRY(sync(h, "tile arrays"));
+    dfree(p);
+    p = q;
+    capacity = nc;
+    return RISQGPU_OK;
+}
+
+}  // namespace
+
+int tile_shape(int64_t N, int& rb, int& cb) {
+    rb = 9;   // 512 rows per panel
+    cb = 12;  // 4096 columns per window
+    while (cb < 16 && ((N + ((int64_t)1 << cb) - 1) >> cb) > MAX_BINS) cb++;
+    return ((N + ((int64_t)1 << cb) - 1) >> cb) <= MAX_BINS ? RISQGPU_OK : RISQGPU_ERR_INVALID;
+}
+
+int TileBuilder::begin(risqgpu* h_, int64_t n_panels) {
+    h = h_;
+    const int64_t N = (int64_t)h->N;
+    free_tiles(h);
+    h->n_panels = n_panels;
+    RQ_TRY(dalloc(h, h->d_panel_tile, (size_t)n_panels + 1));
+    RQ_TRY(dalloc(h, h->d_left_off, (size_t)N));
+    RQ_TRY(dalloc(h, h->d_left_len, (size_t)N));
+    RQ_TRY(dalloc(h, row_abs, (size_t)N));
+    RQ_TRY(dalloc(h, absmax, 1));
+    RQ_CUDA(h, cudaMemsetAsync(row_abs, 0, sizeof(float) * N, h->stream));
+    RQ_CUDA(h, cudaMemsetAsync(absmax, 0, sizeof(unsigned int), h->stream));
+    tile_cap = 0;
+    el_next = tile_next = 0;
+    return RISQGPU_OK;
+}
+
+template <typename VIN>
+int TileBuilder::chunk(int64_t p_lo, int64_t p_hi, const int64_t* row_start, int64_t base, const int32_t* row_len,
+                       const int32_t* cols, const VIN* vin, const float* vlo_in, VIN* vout, float* vlo_out) {
+    const int64_t N = (int64_t)h->N;
+    const int64_t np = p_hi - p_lo;
+    if (np <= 0) return RISQGPU_OK;
+    int64_t *nel = nullptr, *ndense = nullptr, *el_off = nullptr, *t_off = nullptr, *nt64 = nullptr;
+    int32_t* nt = nullptr;
+    char* tmp = nullptr;
+    ScopedFree<7> release(nel, ndense, el_off, t_off, nt64, nt, tmp);
+    RQ_TRY(dalloc(h, nel, np));
+    RQ_TRY(dalloc(h, ndense, np));
+    RQ_TRY(dalloc(h, el_off, np));
+    RQ_TRY(dalloc(h, t_off, np));
+    RQ_TRY(dalloc(h, nt64, np));
+    RQ_TRY(dalloc(h, nt, np));
+    const int rb = h->tile_rb, cb = h->tile_cb;
+    const size_t smem_count = sizeof(int32_t) * MAX_BINS;
+    const size_t smem_scatter = sizeof(int32_t) * (MAX_BINS + ((size_t)1 << rb));
+    RQ_CUDA(h, cudaFuncSetAttribute(k_tile_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_count));
+    RQ_CUDA(h, cudaFuncSetAttribute(k_tile_scatter<VIN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem_scatter));
+    const int grid = (int)std::min<int64_t>(np, (int64_t)num_sms(h) * 2);
+    k_tile_count<<<grid, TT, smem_count, h->stream>>>(N, p_lo, p_hi, rb, cb, row_start, base, row_len, cols, nel,
+                                                      ndense, nt, h->d_left_len);
+    RQ_TRY(check_launch(h, "tile count"));
+    k_widen<<<grid_n(h, np), 256, 0, h->stream>>>(nt, np, nt64);
+    size_t tb1 = 0, tb2 = 0;
+    cub::DeviceScan::ExclusiveScan(nullptr, tb1, nel, el_off, cub::Sum(), (int64_t)el_next, (int)np, h->stream);
+    cub::DeviceScan::ExclusiveScan(nullptr, tb2, nt64, t_off, cub::Sum(), (int64_t)tile_next, (int)np, h->stream);
+    RQ_TRY(dalloc(h, tmp, std::max(tb1, tb2)));
+    cub::DeviceScan::ExclusiveScan(tmp, tb1, nel, el_off, cub::Sum(), (int64_t)el_next, (int)np, h->stream);
+    cub::DeviceScan::ExclusiveScan(tmp, tb2, nt64, t_off, cub::Sum(), (int64_t)tile_next, (int)np, h->stream);
+    RQ_TRY(check_launch(h, "tile offsets"));
+    int64_t last[4];
+    RQ_CUDA(h, cudaMemcpyAsync(last + 0, el_off + np - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_CUDA(h, cudaMemcpyAsync(last + 1, nel + np - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_CUDA(h, cudaMemcpyAsync(last + 2, t_off + np - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_CUDA(h, cudaMemcpyAsync(last + 3, nt64 + np - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "tile offsets"));
+    const int64_t el_end = last[0] + last[1], t_end = last[2] + last[3];
+    size_t c1 = tile_cap, c2 = tile_cap, c3 = tile_cap;
+    RQ_TRY(grow(h, h->d_tile_win, c1, (size_t)t_end, (size_t)tile_next));
+    RQ_TRY(grow(h, h->d_tile_len, c2, (size_t)t_end, (size_t)tile_next));
+    RQ_TRY(grow(h, h->d_tile_off, c3, (size_t)t_end, (size_t)tile_next));
+    tile_cap = c1;
+    RQ_CUDA(h, cudaMemcpyAsync(h->d_panel_tile + p_lo, t_off, sizeof(int64_t) * np, cudaMemcpyDeviceToDevice,
+                               h->stream));
+    k_tile_scatter<VIN><<<grid, TT, smem_scatter, h->stream>>>(
+        N, p_lo, p_hi, rb, cb, row_start, base, row_len, cols, vin, vlo_in, el_off, t_off, ndense, h->d_left_len,
+        h->d_tile_win, h->d_tile_len, h->d_tile_off, h->d_left_off, h->d_el_idx, vout, vlo_out, row_abs);
+    RQ_TRY(check_launch(h, "tile scatter"));
+    RQ_TRY(sync(h, "tile scatter"));
+    el_next = el_end;
+    tile_next = t_end;
+    return RISQGPU_OK;
+}
+
+int TileBuilder::finish() {
+    const int64_t N = (int64_t)h->N;
+    RQ_CUDA(h, cudaMemcpyAsync(h->d_panel_tile + h->n_panels, &tile_next, sizeof(int64_t), cudaMemcpyHostToDevice,
+                               h->stream));
+    k_max_f32<<<grid_n(h, N), 256, 0, h->stream>>>(row_abs, N, absmax);
+    unsigned int bits = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&bits, absmax, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "row sums"));
+    float m;
+    std::memcpy(&m, &bits, sizeof(m));
+    // FP32 sums of |H|: a relative margin covers their rounding
+    h->h_row_abs_max = 1.01 * (double)m;
+    h->n_tiles = tile_next;
+    h->n_dense_el = 0;
+    if (tile_next > 0) {
+        int64_t* sum = nullptr;
+        char* tmp = nullptr;
+        ScopedFree<2> release(sum, tmp);
+        RQ_TRY(dalloc(h, sum, 1));
+        size_t tb = 0;
+        cub::DeviceReduce::Sum(nullptr, tb, h->d_tile_len, sum, (int)tile_next, h->stream);
+        RQ_TRY(dalloc(h, tmp, tb));
+        cub::DeviceReduce::Sum(tmp, tb, h->d_tile_len, sum, (int)tile_next, h->stream);
+        int64_t v = 0;
+        RQ_CUDA(h, cudaMemcpyAsync(&v, sum, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+        RQ_TRY(sync(h, "dense pairs"));
+        h->n_dense_el = (uint64_t)v;
+    }
+    RQ_TRY(dalloc(h, h->d_acc, (size_t)N));
+    RQ_TRY(dalloc(h, h->d_sig_scalars, 4));
+    dfree(row_abs);
+    dfree(absmax);
+    h->tiled = true;
+    return RISQGPU_OK;
+}
+
+TileBuilder::~TileBuilder() {
+    dfree(row_abs);
+    dfree(absmax);
+}
+
+template int TileBuilder::chunk<double>(int64_t, int64_t, const int64_t*, int64_t, const int32_t*, const int32_t*,
+                                        const double*, const float*, double*, float*);
+template int TileBuilder::chunk<float>(int64_t, int64_t, const int64_t*, int64_t, const int32_t*, const int32_t*,
+                                       const float*, const float*, float*, float*);
+
+// sigma over tiled storage; kind 0: FP64 vectors (FP64 values, or FP32 + remainder),
+// 1: FP32 vectors with the FP32 values.
+int sigma_tiles(risqgpu* h, const void* x, void* y, int kind) {
+    if (kind == 0) {
+        if (h->precision == RISQGPU_FP64)
+            return launch_tiles<double, double, false>(h, (const double*)x, (double*)y, h->d_val64, nullptr);
+        if (h->precision == RISQGPU_MIXED)
+            return launch_tiles<float, double, true>(h, (const double*)x, (double*)y, h->d_val32, h->d_val_lo);
+        h->err = "FP64 sigma needs FP64 or FP32 + remainder values";
+        return RISQGPU_ERR_INVALID;
+    }
+    if (h->precision == RISQGPU_FP64) {
+        h->err = "FP32 sigma needs FP32 values";
+        return RISQGPU_ERR_INVALID;
+    }
+    return launch_tiles<float, float, false>(h, (const float*)x, (float*)y, h->d_val32, nullptr);
+}
+
+// Every stored pair of a tiled build as (p, q, value), internal indices, in storage order
+// (nnz_upper entries each).
+int tiles_coo(risqgpu* h, int32_t* p, int32_t* q, double* v) { return tiles_each(h, CooOut{p, q, v}); }
+
+// out[i] -= sum_j H_ij^2 / max(H_jj - E, gmin) over the stored pairs (out zeroed by the caller).
+int tiles_self_energy(risqgpu* h, double energy, double gmin, double* out) {
+    return tiles_each(h, SelfEnergyAdd{h->d_diag, energy, gmin, out});
+}
+
+int tiles_rows(risqgpu* h, const uint32_t* mark, int64_t* out_r, int64_t* out_c, double* out_v,
+               unsigned long long* count, unsigned long long cap) {
+    return tiles_each(h, RowFilter{mark, h->d_orig, out_r, out_c, out_v, count, cap});
+}
+
+void free_tiles(risqgpu* h) {
+    dfree(h->d_panel_tile);
+    dfree(h->d_tile_win);
+    dfree(h->d_tile_len);
+    dfree(h->d_tile_off);
+    dfree(h->d_left_off);
+    dfree(h->d_left_len);
+    dfree(h->d_el_idx);
+    dfree(h->d_acc);
+    dfree(h->d_sig_scalars);
+    h->tiled = false;
+    h->n_panels = h->n_tiles = 0;
+    h->n_dense_el = 0;
+    h->h_row_abs_max = 0.0;
+}
+
+}  // namespace risq

@@ -116,6 +116,21 @@ class GpuHam:
                                              nu, A.ptr(diag, A._dp)), self._h)
         return rp, cols[:nu], vals[:nu], diag
 
+    def export_rows(self, rows, cap=None):
+        """Stored elements of the given caller rows in both triangles: arrays (row, col, val)
+        in no particular order (risqgpu_export_rows)."""
+        r = np.ascontiguousarray(rows, dtype=np.int64)
+        if cap is None:
+            cap = max(1, 20000 * len(r))
+        out_r = np.zeros(cap, dtype=np.int64)
+        out_c = np.zeros(cap, dtype=np.int64)
+        out_v = np.zeros(cap)
+        cnt = C.c_size_t()
+        A.check(A.lib().risqgpu_export_rows(self._h, A.ptr(r, A._i64p), len(r), A.ptr(out_r, A._i64p),
+                                            A.ptr(out_c, A._i64p), A.ptr(out_v, A._dp), cap, C.byref(cnt)), self._h)
+        k = cnt.value
+        return out_r[:k], out_c[:k], out_v[:k]
+
     def matrix_vector_prod(self, x) -> np.ndarray:
         x = np.ascontiguousarray(x, dtype=np.float64)
         if x.size != self.n:
@@ -201,6 +216,23 @@ class GpuHam:
         A.lib().risqgpu_var_log(self._h, recs, k.value, C.byref(k))
         self.n = N
         return e.value, d, c, g, [recs[i].as_dict() for i in range(k.value)]
+
+    def set_subspace(self, max_space: int = 0, keep: int = 0):
+        """Davidson search space and restart size of this handle's solves; (0, 0) is the
+        reference's nroots + 10 with a restart to the nroots Ritz vectors
+        (risqgpu_set_subspace)."""
+        A.check(A.lib().risqgpu_set_subspace(self._h, int(max_space), int(keep)), self._h)
+
+    def set_memory_limit(self, nbytes: int):
+        """Bound the device memory the handle may hold (0 = no bound); allocations past it
+        fail with ERR_OOM (risqgpu_set_memory_limit)."""
+        A.check(A.lib().risqgpu_set_memory_limit(self._h, int(nbytes)), self._h)
+
+    def memory_used(self):
+        """(bytes held by the handle, its bound or 0)."""
+        u, l = C.c_size_t(), C.c_size_t()
+        A.check(A.lib().risqgpu_memory_used(self._h, C.byref(u), C.byref(l)), self._h)
+        return u.value, l.value
 
     def set_stream(self, stream_ptr):
         """Issue the handle's work on a caller cudaStream_t (int address); None = own stream."""

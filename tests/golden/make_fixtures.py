@@ -1,7 +1,7 @@
 """Generate the committed golden fixtures from the reference checkout.
 
-Run in a container that has the reference mounted (default /root/reference):
-    python tests/golden/make_fixtures.py [/path/to/reference]
+Run in a container that has the reference checkout, giving its path:
+    python tests/golden/make_fixtures.py /path/to/reference
 
 For each example system with a pinned variational energy in the reference's
 integration tests (tests/integration_test_suite.rs:28-93) this stores the
@@ -57,4 +57,6 @@ def main(ref: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_fixtures.py /path/to/reference")
+    main(sys.argv[1])

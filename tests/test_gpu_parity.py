@@ -250,8 +250,9 @@ def test_columns_only_build_and_recomputed_sigma(name):
 
 @pytest.mark.parametrize("name", ["be2", "f2"])
 def test_upper_triangle_storage(name):
-    """FP64_UPPER / MIXED_UPPER store each pair once (SparseMatUpperTri's layout) and
-    add the transposed half with atomics: same set and values, same sigma to rounding."""
+    """FP64_UPPER / MIXED_UPPER store each pair once (SparseMatUpperTri's layout),
+    regrouped into row-panel x column-window tiles: same set and values as the
+    both-triangle build, same sigma to rounding."""
     ints, p = H.golden_system(name)
     _, dets, coeffs, diag, _ = H.oracle_hci(name)
     x = np.random.default_rng(9).standard_normal(len(dets))
@@ -282,9 +283,9 @@ def test_upper_triangle_storage(name):
 
 
 def test_upper_triangle_sigma_on_large_alpha_groups():
-    """The blocked upper-triangle sigma on a set whose alpha groups exceed both the
-    1024-column window and the 256-row work item (n20 8a8b, eps 1e-3): FP64 against
-    the both-triangle kernel (checked against the oracle above), FP32 and the FP32 +
+    """Upper-triangle sigma on a set whose alpha groups hold more than 1024
+    determinants (n20 8a8b, eps 1e-3, 551,147 determinants): FP64 against the
+    both-triangle kernel (checked against the oracle above), FP32 and the FP32 +
     remainder storage against the same reference."""
     from risq_b200.fcidump import synthetic_integrals
     ints = synthetic_integrals(20, 0)
@@ -292,7 +293,7 @@ def test_upper_triangle_sigma_on_large_alpha_groups():
         e, dets, c, diag, log = g.variational(8, 8, 1e-3, dav_max_iter=2000)
         up = dets[:, 0]
         _, counts = np.unique(up, return_counts=True)
-        assert counts.max() > 1024  # windows are split and groups span several work items
+        assert counts.max() > 1024  # groups larger than a warp's and a block's share of rows
         x = np.random.default_rng(3).standard_normal(len(dets))
         g.set_dets(dets, 0, diag)
         g.build(_capi.FP64)

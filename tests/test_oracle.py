@@ -165,3 +165,22 @@ def test_dense_davidson_two_roots():
     rc, ev, vec, st = O.davidson_dense(A, 2, None, 1e-8, 1e-12, 200)
     assert rc == 0
     np.testing.assert_allclose(ev, np.linalg.eigvalsh(A)[:2], atol=1e-9)
+
+
+def test_parallel_oracle_matches_serial():
+    # the multi-threaded build and sigma of the CPU baseline: the serial fast builder's
+    # pairs and values, and the same energy
+    _, dets, coeffs, diag, _ = H.oracle_hci("f2")
+    ints, p = H.golden_system("f2")
+    ham = H.oracle_ham(ints, p["norb_core"])
+    s1 = O.Sparse().build(ham, dets, diag, 0, builder=1)
+    s2 = O.Sparse().build_par(ham, dets, diag)
+    for a, b in zip(s1.export(), s2.export()):
+        assert np.array_equal(a, b)
+    x = np.random.default_rng(5).standard_normal(len(dets))
+    y1, y2 = s1.mv(x), s2.mv_par(x)
+    assert np.max(np.abs(y1 - y2)) <= 1e-12 * np.max(np.abs(y1))
+    r1 = s1.davidson(1, coeffs, 1e-4, 1e-8, 200)
+    r2 = s2.davidson(1, coeffs, 1e-4, 1e-8, 200, parallel=True)
+    assert r1[0] == 0 and r2[0] == 0
+    assert abs(r1[1][0] - r2[1][0]) < 1e-10
