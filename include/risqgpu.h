@@ -217,6 +217,25 @@ RISQGPU_API int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs,
  * keep <= max_space / 2. */
 RISQGPU_API int risqgpu_set_subspace(risqgpu_t* h, int max_space, int keep);
 
+/* All-reduce supplied by a multi-GPU caller: sum `count` int64 values at device
+ * address buf_dev in place across the ranks, ordered after the work already issued on
+ * `stream` (a cudaStream_t) and before the work issued there after the call returns;
+ * return 0 on success.  Every rank calls it at the same points with the same count. */
+typedef int (*risqgpu_allreduce_fn)(void* buf_dev, size_t count, void* stream, void* user);
+
+/* Row-block partition of the upper-triangle storage for nranks GPUs (one handle and one
+ * process per GPU, every rank holding the same determinant set).  The next upper-triangle
+ * build of this handle (FP64_UPPER, FP32_UPPER or MIXED_UPPER) stores only rank `rank`'s
+ * share of the row panels (contiguous panels cut so that the shares hold equal numbers of
+ * pairs), and every sigma sums this share into 64-bit fixed-point partial sums that
+ * `reduce` adds across the ranks; integer sums are exact, so every rank gets the sigma of
+ * the whole matrix, bitwise equal to a single-GPU build's, and the replicated Davidson
+ * solves on the ranks stay identical.  The reference is single-threaded and has no
+ * counterpart (its matrix_vector_prod, src/var/sparse.rs:64-78, splits naturally by rows).
+ * nranks = 1 (reduce may be NULL) restores the undivided build.  Statistics and
+ * risqgpu_nnz then count this rank's pairs. */
+RISQGPU_API int risqgpu_set_partition(risqgpu_t* h, int rank, int nranks, risqgpu_allreduce_fn reduce, void* user);
+
 /* Bound the device memory this handle may hold (bytes; 0 = no bound beyond the
  * device).  An allocation past the bound fails with RISQGPU_ERR_OOM, as a failed
  * cudaMalloc would, and leaves the handle usable.  No counterpart in the reference:

@@ -86,6 +86,8 @@ def lib():
         L.or_hci_new.restype = C.c_void_p
         L.or_hci_new.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int]
         L.or_hci_free.argtypes = [C.c_void_p]
+        L.or_hci_step_bounded.argtypes = [C.c_void_p, C.c_size_t]
+        L.or_hci_step_bounded.restype = C.c_int
         L.or_hci_step.argtypes = [C.c_void_p]
         L.or_hci_step.restype = C.c_int
         L.or_hci_run.argtypes = [C.c_void_p, C.c_int]
@@ -332,6 +334,11 @@ class Hci:
 
     def step(self) -> bool:
         return bool(lib().or_hci_step(self.ptr))
+
+    def step_bounded(self, max_dets) -> int:
+        """One iteration unless its selection takes the space past max_dets: 0 done, 1 converged,
+        2 stopped after the selection (the state then only serves the earlier export)."""
+        return int(lib().or_hci_step_bounded(self.ptr, int(max_dets)))
 
     @property
     def energy(self):

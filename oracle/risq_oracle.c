@@ -1772,6 +1772,28 @@ OR_EXPORT int or_hci_step(Hci *H) {
     return 0;
 }
 
+/* One loop pass that stops after the selection when the space would exceed max_dets:
+ * returns 2 then (the new determinants are appended but not optimised, so the state
+ * is only good for reading the earlier space, exported before the call). */
+OR_EXPORT int or_hci_step_bounded(Hci *H, size_t max_dets) {
+    int none = find_new_dets(H);
+    if (H->eps == H->eps_var && none) { H->converged = 1; return 1; }
+    if (H->wf.n > max_dets) return 2;
+    int it = H->nlog + 1;
+    int ds[4] = {0};
+    sparse_optimize(H, 1e-4, 1e-8, it > 1, ds);
+    if (H->nlog < 64) {
+        H->log_eps[H->nlog] = H->eps;
+        H->log_energy[H->nlog] = H->wf.energy;
+        H->log_ndets[H->nlog] = H->wf.n;
+        H->log_nnz[H->nlog] = or_sparse_nnz(H->sp);
+        memcpy(H->log_dav[H->nlog], ds, sizeof(ds));
+        H->nlog++;
+    }
+    H->eps = eps_next(&H->eps_iter); /* var/mod.rs:123 */
+    return 0;
+}
+
 /* variational (src/var/mod.rs:59-134): at most 20 iterations. */
 OR_EXPORT double or_hci_run(Hci *H, int max_iter) {
     int iter = 0;

@@ -64,6 +64,9 @@ class VarIter(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+# risqgpu_allreduce_fn: int (*)(void* buf_dev, size_t count, void* stream, void* user)
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p)
+
 _dp = C.POINTER(C.c_double)
 _fp = C.POINTER(C.c_float)
 _u64p = C.POINTER(C.c_uint64)
@@ -90,6 +93,7 @@ SIGNATURES = [
     ("risqgpu_sparse_optimize", C.c_int, [_handle, _dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                           _dp, _dp, C.POINTER(HStats), C.POINTER(DStats)]),
     ("risqgpu_set_subspace", C.c_int, [_handle, C.c_int, C.c_int]),
+    ("risqgpu_set_partition", C.c_int, [_handle, C.c_int, C.c_int, ALLREDUCE_FN, C.c_void_p]),
     ("risqgpu_set_memory_limit", C.c_int, [_handle, C.c_size_t]),
     ("risqgpu_memory_used", C.c_int, [_handle, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     ("risqgpu_set_stream", C.c_int, [_handle, C.c_void_p]),

@@ -876,30 +876,49 @@ int fill_tiled(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int p
         RQ_CUDA(h, cudaMemcpyAsync(ps.data(), dps, sizeof(int64_t) * (np + 1), cudaMemcpyDeviceToHost, h->stream));
         RQ_TRY(sync(h, "panel starts"));
     }
+    // this handle's panels: all of them, or with a row-block partition the rank's share,
+    // contiguous panels cut where the counted pairs reach rank / nranks of the total
+    int64_t own_lo = 0, own_hi = np;
+    if (h->part_n > 1) {
+        auto cut = [&](int r) -> int64_t {
+            const int64_t goal = (int64_t)((double)ps[np] * r / h->part_n);
+            return (int64_t)(std::lower_bound(ps.begin(), ps.end() - 1, goal) - ps.begin());
+        };
+        own_lo = h->part_rank == 0 ? 0 : cut(h->part_rank);
+        own_hi = h->part_rank == h->part_n - 1 ? np : cut(h->part_rank + 1);
+        own_hi = std::max(own_hi, own_lo);
+        // rows of other ranks' panels hold no stored pairs here
+        RQ_CUDA(h, cudaMemsetAsync(h->d_row_len, 0, sizeof(int32_t) * n, h->stream));
+    }
+    h->part_p_lo = own_lo;
+    h->part_p_hi = own_hi;
+    const int64_t own_cap = ps[own_hi] - ps[own_lo];
     const size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_MIXED ? 8 : 4);
     const size_t per_el = 4 + vb;
-    // bytes held besides the element arrays: per-row tile data, accumulators, margin
-    const size_t fixed = (size_t)cap * per_el + (size_t)n * 32 + ((size_t)256 << 20);
+    // bytes held besides the element arrays: per-row tile data and accumulators, plus a
+    // margin for the conversion's work buffers that grows with the set (at most 256 MiB)
+    const size_t base_need = (size_t)own_cap * per_el + (size_t)n * 32;
+    const size_t fixed = base_need + std::max((size_t)8 << 20, std::min((size_t)256 << 20, base_need / 32));
     const size_t avail = mem_available(h);
     // chunks: the fewest whose largest chunk fits beside the tiled arrays
     std::vector<int64_t> cuts;
     int64_t max_chunk = 0;
+    const int64_t own_np = own_hi - own_lo;
     for (int64_t K = 1;; K = K < 8 ? K + 1 : K * 2) {
-        const int64_t target = (cap + K - 1) / K;
-        cuts.assign(1, 0);
+        const int64_t target = (own_cap + K - 1) / K;
+        cuts.assign(1, own_lo);
         max_chunk = 0;
-        int64_t start = 0;
-        for (int64_t P = 1; P <= np; P++) {
-            const bool last = P == np;
+        int64_t start = own_lo;
+        for (int64_t P = own_lo + 1; P <= own_hi; P++) {
+            const bool last = P == own_hi;
             if (last || ps[P + 1] - ps[start] > target) {
-                if (!last && P == start) continue;
                 cuts.push_back(P);
                 max_chunk = std::max(max_chunk, ps[P] - ps[start]);
                 start = P;
             }
         }
         if (fixed + (size_t)max_chunk * per_el <= avail) break;
-        if (K >= np) {
+        if (K >= own_np) {
             h->err = "tiled upper-triangle H needs " + std::to_string((fixed + (size_t)max_chunk * per_el) >> 20) +
                      " MiB, " + std::to_string(avail >> 20) + " MiB available";
             return RISQGPU_ERR_OOM;
@@ -909,16 +928,16 @@ int fill_tiled(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int p
     double* c64 = nullptr;
     float *c32 = nullptr, *clo = nullptr;
     ScopedFree<4> release(ccols, c64, c32, clo);
-    RQ_TRY(dalloc(h, h->d_el_idx, (size_t)cap));
-    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, (size_t)cap));
-    else RQ_TRY(dalloc(h, h->d_val32, (size_t)cap));
-    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, (size_t)cap));
+    RQ_TRY(dalloc(h, h->d_el_idx, (size_t)own_cap));
+    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, (size_t)own_cap));
+    else RQ_TRY(dalloc(h, h->d_val32, (size_t)own_cap));
+    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, (size_t)own_cap));
     RQ_TRY(dalloc(h, ccols, (size_t)max_chunk));
     if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, c64, (size_t)max_chunk));
     else RQ_TRY(dalloc(h, c32, (size_t)max_chunk));
     if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, clo, (size_t)max_chunk));
     TileBuilder tb;
-    RQ_TRY(tb.begin(h, np));
+    RQ_TRY(tb.begin(h, np, own_cap));
     for (size_t c = 0; c + 1 < cuts.size(); c++) {
         const int64_t p_lo = cuts[c], p_hi = cuts[c + 1];
         const int64_t r_lo = p_lo << rb, r_hi = std::min(n, p_hi << rb);
@@ -933,7 +952,25 @@ int fill_tiled(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int p
             RQ_TRY(tb.chunk<float>(p_lo, p_hi, h->d_row_start, base, h->d_row_len, ccols, c32, clo, h->d_val32,
                                    h->d_val_lo));
     }
-    return tb.finish();
+    RQ_TRY(tb.finish());
+    // every stored element went into the tiles exactly once
+    int64_t* sum = nullptr;
+    char* tmp = nullptr;
+    ScopedFree<2> release_sum(sum, tmp);
+    RQ_TRY(dalloc(h, sum, 1));
+    size_t tbytes = 0;
+    cub::DeviceReduce::Sum(nullptr, tbytes, h->d_row_len, sum, (int)n, h->stream);
+    RQ_TRY(dalloc(h, tmp, tbytes));
+    cub::DeviceReduce::Sum(tmp, tbytes, h->d_row_len, sum, (int)n, h->stream);
+    int64_t stored = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&stored, sum, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "tiled count check"));
+    if (stored != tb.el_next) {
+        h->err = "tiled layout holds " + std::to_string(tb.el_next) + " elements for " + std::to_string(stored) +
+                 " stored";
+        return RISQGPU_ERR_INVALID;
+    }
+    return RISQGPU_OK;
 }
 
 // stored count, statistics and handle state after a fill
@@ -1047,7 +1084,8 @@ int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats*
     {
         // refuse up front when the rows cannot be stored, leaving the handle unchanged
         size_t vb = precision == RISQGPU_FP64 ? 8 : (precision == RISQGPU_FP32 ? 4 : (precision == RISQGPU_COLS ? 0 : 8));
-        size_t need = (size_t)cap * (4 + vb) + ((size_t)64 << 20);
+        const size_t arrays = (size_t)cap * (4 + vb);
+        size_t need = arrays + std::max((size_t)8 << 20, std::min((size_t)64 << 20, arrays / 16));
         const size_t fr = mem_available(h);
         if (need > fr) {
             h->err = "sparse H needs " + std::to_string(need >> 20) + " MiB, " + std::to_string(fr >> 20) +

@@ -221,6 +221,19 @@ int risqgpu_set_subspace(risqgpu_t* h, int max_space, int keep) {
     return RISQGPU_OK;
 }
 
+int risqgpu_set_partition(risqgpu_t* h, int rank, int nranks, risqgpu_allreduce_fn reduce, void* user) {
+    if (!h) return RISQGPU_ERR_INVALID;
+    if (nranks < 1 || rank < 0 || rank >= nranks || (nranks > 1 && !reduce)) {
+        h->err = "partition needs 0 <= rank < nranks and, for nranks > 1, a reduce function";
+        return RISQGPU_ERR_INVALID;
+    }
+    h->part_rank = rank;
+    h->part_n = nranks;
+    h->part_reduce = nranks > 1 ? reduce : nullptr;
+    h->part_user = user;
+    return RISQGPU_OK;
+}
+
 int risqgpu_set_memory_limit(risqgpu_t* h, size_t bytes) {
     if (!h) return RISQGPU_ERR_INVALID;
     h->mem_limit = bytes;

@@ -130,6 +130,14 @@ struct risqgpu {
     long long* d_acc = nullptr;
     double* d_sig_scalars = nullptr;
 
+    // Row-block partition for several GPUs (risqgpu_set_partition): this handle builds
+    // and applies the row panels [part_p_lo, part_p_hi) of the tiled layout; partial
+    // sums are added across the ranks by the caller's all-reduce.
+    int part_rank = 0, part_n = 1;
+    risqgpu_allreduce_fn part_reduce = nullptr;
+    void* part_user = nullptr;
+    int64_t part_p_lo = 0, part_p_hi = 0;
+
     // previous build kept for an incremental extension
     size_t prev_N = 0;
     int32_t* d_prev_orig = nullptr;
@@ -268,6 +276,9 @@ int permute_out(risqgpu* h, const double* yi, double* y);
 // tiled upper-triangle storage (tiles.cu)
 int tile_shape(int64_t N, int& rb, int& cb);
 int sigma_tiles(risqgpu* h, const void* x, void* y, int kind);
+// Sum `count` int64 values in place across the partition's ranks (the caller's all-reduce,
+// on the handle's stream).
+int part_allreduce(risqgpu* h, void* buf_dev, size_t count);
 int tiles_coo(risqgpu* h, int32_t* p, int32_t* q, double* v);
 int tiles_self_energy(risqgpu* h, double energy, double gmin, double* out);
 int tiles_rows(risqgpu* h, const uint32_t* mark, int64_t* out_r, int64_t* out_c, double* out_v,
@@ -279,11 +290,12 @@ void free_tiles(risqgpu* h);
 // arrays (d_el_idx and the value arrays must already hold room for every element).
 struct TileBuilder {
     risqgpu* h = nullptr;
-    float* row_abs = nullptr;       // N: sum_q |H_pq| over both triangles
-    unsigned int* absmax = nullptr;
+    unsigned long long* row_abs = nullptr;  // N: sum_q |H_pq| over both triangles, units of 2^-32
+    unsigned long long* absmax = nullptr;
     size_t tile_cap = 0;
+    int64_t el_cap = 0;
     int64_t el_next = 0, tile_next = 0;
-    int begin(risqgpu* h, int64_t n_panels);
+    int begin(risqgpu* h, int64_t n_panels, int64_t element_capacity);
     template <typename VIN>
     int chunk(int64_t p_lo, int64_t p_hi, const int64_t* row_start, int64_t base, const int32_t* row_len,
               const int32_t* cols, const VIN* vin, const float* vlo_in, VIN* vout, float* vlo_out);

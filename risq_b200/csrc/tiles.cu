@@ -121,7 +121,9 @@ __global__ void __launch_bounds__(TT) k_tile_count(int64_t N, int64_t p_lo, int6
 
 // Scatter the chunk's pairs into the tiled arrays.  panel_el_off / panel_tile_off:
 // absolute first element / first tile of every panel of the chunk.  Also adds |H_pq|
-// to the row sums of both p and q (row_abs, for the fixed-point scale).
+// to the row sums of both p and q (row_abs, in units of 2^-32: integer sums are exact,
+// so the sums and the fixed-point scale derived from them do not depend on the order
+// of the additions, nor on how the rows are split between ranks).
 template <typename VIN>
 __global__ void __launch_bounds__(TT) k_tile_scatter(
     int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb, const int64_t* __restrict__ row_start, int64_t base,
@@ -130,7 +132,8 @@ __global__ void __launch_bounds__(TT) k_tile_scatter(
     const int64_t* __restrict__ panel_tile_off, const int64_t* __restrict__ panel_dense_el,
     const int32_t* __restrict__ left_len, int32_t* __restrict__ tile_win, int32_t* __restrict__ tile_len,
     int64_t* __restrict__ tile_off, int64_t* __restrict__ left_off, uint32_t* __restrict__ el_idx,
-    VIN* __restrict__ vout, float* __restrict__ vlo_out, float* __restrict__ row_abs) {
+    VIN* __restrict__ vout, float* __restrict__ vlo_out, unsigned long long* __restrict__ row_abs, int64_t el_cap,
+    int64_t tile_cap) {
     extern __shared__ int32_t sm_i[];
     int32_t* cursor = sm_i;              // per window: next dense slot (panel-relative), or -1
     int32_t* lcur = sm_i + MAX_BINS;     // per row of the panel: leftover start (panel-relative)
@@ -174,9 +177,11 @@ __global__ void __launch_bounds__(TT) k_tile_scatter(
         for (int b = b_lo; b < b_hi; b++) {
             const int c = cursor[b];
             if (c > 0 && dense_tile(c, window_width(N, J0 + b, cb))) {
-                tile_win[t0 + ex_t] = (int32_t)(J0 + b);
-                tile_len[t0 + ex_t] = c;
-                tile_off[t0 + ex_t] = el0 + ex_el;
+                if (t0 + ex_t < tile_cap) {  // always true: the count pass sized the tile arrays
+                    tile_win[t0 + ex_t] = (int32_t)(J0 + b);
+                    tile_len[t0 + ex_t] = c;
+                    tile_off[t0 + ex_t] = el0 + ex_el;
+                }
                 cursor[b] = (int32_t)ex_el;
                 ex_el += c;
                 ex_t++;
@@ -205,7 +210,7 @@ __global__ void __launch_bounds__(TT) k_tile_scatter(
             const int len = row_len[r];
             const uint32_t lr = (uint32_t)(r - r0);
             int lnext = lcur[lr];
-            float rsum = 0.f;
+            unsigned long long rsum = 0ull;
             for (int k0 = 0; k0 < len; k0 += 32) {
                 const int k = k0 + lane;
                 const bool act = k < len;
@@ -217,6 +222,15 @@ __global__ void __launch_bounds__(TT) k_tile_scatter(
                 }
                 const bool left = act && cur < 0;
                 const unsigned ml = __ballot_sync(FULL, left);
+                // this row's pairs that fall in one dense tile take consecutive slots, so
+                // that sigma meets them as runs of one row
+                const bool dense = act && !left;
+                const int bin = (int)((q >> cb) - J0);
+                const unsigned grp = __match_any_sync(FULL, dense ? bin : (int)(0x80000000u | (unsigned)lane));
+                const int leader = __ffs(grp) - 1;
+                int slot = 0;
+                if (dense && lane == leader) slot = atomicAdd(&cursor[bin], __popc(grp));
+                slot = __shfl_sync(FULL, slot, leader);
                 int64_t pos = 0;
                 uint32_t code = 0;
                 if (act) {
@@ -224,25 +238,29 @@ __global__ void __launch_bounds__(TT) k_tile_scatter(
                         pos = el0 + lnext + __popc(ml & lt);
                         code = (uint32_t)q;
                     } else {
-                        pos = el0 + atomicAdd(&cursor[(q >> cb) - J0], 1);
+                        pos = el0 + slot + __popc(grp & lt);
                         code = (lr << cb) | ((uint32_t)q & cmask);
                     }
-                    el_idx[pos] = code;
                     const VIN v = vin[s + k];
-                    vout[pos] = v;
-                    float av = fabsf((float)v);
-                    if (vlo_in) {
-                        vlo_out[pos] = vlo_in[s + k];
-                        av = (float)fabs((double)v + (double)vlo_in[s + k]);
+                    const bool in = pos >= 0 && pos < el_cap;  // always true: see the count pass
+                    if (in) {
+                        el_idx[pos] = code;
+                        vout[pos] = v;
                     }
-                    rsum += av;
-                    atomicAdd(row_abs + q, av);
+                    double av = fabs((double)v);
+                    if (vlo_in) {
+                        if (in) vlo_out[pos] = vlo_in[s + k];
+                        av = fabs((double)v + (double)vlo_in[s + k]);
+                    }
+                    const unsigned long long ai = (unsigned long long)llrint(av * 4294967296.0);
+                    rsum += ai;
+                    atomicAdd(row_abs + q, ai);
                 }
                 lnext += __popc(ml);
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) rsum += __shfl_xor_sync(FULL, rsum, o);
-            if (lane == 0) atomicAdd(row_abs + r, rsum);
+            if (lane == 0 && rsum) atomicAdd(row_abs + r, rsum);
         }
         __syncthreads();
     }
@@ -253,13 +271,13 @@ __global__ void k_widen(const int32_t* __restrict__ a, int64_t n, int64_t* __res
         b[i] = a[i];
 }
 
-__global__ void k_max_f32(const float* __restrict__ a, int64_t n, unsigned int* __restrict__ out) {
-    float m = 0.f;
+__global__ void k_max_u64(const unsigned long long* __restrict__ a, int64_t n, unsigned long long* __restrict__ out) {
+    unsigned long long m = 0ull;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        m = fmaxf(m, a[i]);
+        m = max(m, a[i]);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(out, __float_as_uint(m));  // non-negative floats order as integers
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(FULL, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
 // ---------------------------------------------------------------- sigma
@@ -301,10 +319,28 @@ __device__ __forceinline__ void sadd(long long* a, long long v) {
     atomicAdd(reinterpret_cast<unsigned long long*>(a), (unsigned long long)v);
 }
 
+// Four consecutive stored values (16-byte aligned element index e) as the vector type.
+template <typename V, typename X, bool VLO>
+__device__ __forceinline__ void load4(const V* __restrict__ vals, const float* __restrict__ vlo, int64_t e,
+                                      X (&v)[4]) {
+    if constexpr (std::is_same<V, double>::value) {
+        const double2 a = __ldcs(reinterpret_cast<const double2*>(vals + e));
+        const double2 b = __ldcs(reinterpret_cast<const double2*>(vals + e + 2));
+        v[0] = (X)a.x; v[1] = (X)a.y; v[2] = (X)b.x; v[3] = (X)b.y;
+    } else {
+        const float4 a = __ldcs(reinterpret_cast<const float4*>(vals + e));
+        v[0] = (X)a.x; v[1] = (X)a.y; v[2] = (X)a.z; v[3] = (X)a.w;
+        if constexpr (VLO) {
+            const float4 l = __ldcs(reinterpret_cast<const float4*>(vlo + e));
+            v[0] += (X)l.x; v[1] += (X)l.y; v[2] += (X)l.z; v[3] += (X)l.w;
+        }
+    }
+}
+
 // V: stored value type; VLO: add the FP32 remainder (MIXED storage); X: vector type.
 template <typename V, typename X, bool VLO>
 __global__ void __launch_bounds__(TT) k_sigma_tiles(
-    int64_t N, int64_t n_panels, int rb, int cb, const int64_t* __restrict__ panel_tile,
+    int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb, const int64_t* __restrict__ panel_tile,
     const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
     const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len, const uint32_t* __restrict__ el_idx,
     const V* __restrict__ vals, const float* __restrict__ vlo, const X* __restrict__ x,
@@ -321,10 +357,10 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
     const X scale = (X)scalars[1];
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
     for (;;) {
-        if (threadIdx.x == 0) s_panel = (long long)atomicAdd(counter, 1ull);
+        if (threadIdx.x == 0) s_panel = p_lo + (long long)atomicAdd(counter, 1ull);
         __syncthreads();
         const int64_t P = s_panel;
-        if (P >= n_panels) break;
+        if (P >= p_hi) break;
         const int64_t r0 = P << rb;
         const int nr = (int)min((int64_t)R, N - r0);
         for (int i = threadIdx.x; i < nr; i += TT) {
@@ -343,32 +379,46 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
                 yJ[i] = 0;
             }
             __syncthreads();
-            int k = threadIdx.x;
-            for (; k + 3 * TT < len; k += 4 * TT) {
-                uint32_t u[4];
-                X v[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    u[j] = __ldcs(el_idx + e0 + k + j * TT);
-                    v[j] = (X)__ldcs(vals + e0 + k + j * TT);
-                    if constexpr (VLO) v[j] += (X)__ldcs(vlo + e0 + k + j * TT);
+            // the unaligned head and tail one pair per thread, the 16-byte aligned body in
+            // blocks of four consecutive pairs per thread (vector loads, coalesced across the
+            // warp); consecutive pairs of one row add their row sums in a register first
+            const int head = (int)min((int64_t)len, (4 - (e0 & 3)) & 3);
+            const int64_t eb = e0 + head;
+            const int nblk = (len - head) >> 2;
+            const int rest = len - head - 4 * nblk;
+            if ((int)threadIdx.x < head + rest) {
+                const int64_t e = (int)threadIdx.x < head ? e0 + threadIdx.x : eb + 4 * nblk + (threadIdx.x - head);
+                const uint32_t u = __ldcs(el_idx + e);
+                X v = (X)__ldcs(vals + e);
+                if constexpr (VLO) v += (X)__ldcs(vlo + e);
+                const uint32_t lr = u >> cb, lc = u & cmask;
+                if (lr < (uint32_t)nr && lc < (uint32_t)w) {  // never false for a valid layout
+                    sadd(yP + lr, to_fixed<X>(v * xJ[lc], scale));
+                    sadd(yJ + lc, to_fixed<X>(v * xP[lr], scale));
                 }
+            }
+            for (int bk = threadIdx.x; bk < nblk; bk += TT) {
+                const int64_t e = eb + 4 * (int64_t)bk;
+                const uint4 u4 = __ldcs(reinterpret_cast<const uint4*>(el_idx + e));
+                X v[4];
+                load4<V, X, VLO>(vals, vlo, e, v);
+                const uint32_t u[4] = {u4.x, u4.y, u4.z, u4.w};
+                uint32_t rcur = u[0] >> cb;
+                long long racc = 0;
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const uint32_t lr = u[j] >> cb, lc = u[j] & cmask;
                     if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;  // never taken for a valid layout
-                    sadd(yP + lr, to_fixed<X>(v[j] * xJ[lc], scale));
+                    const long long tr = to_fixed<X>(v[j] * xJ[lc], scale);
                     sadd(yJ + lc, to_fixed<X>(v[j] * xP[lr], scale));
+                    if (lr != rcur) {
+                        if (racc != 0 && rcur < (uint32_t)nr) sadd(yP + rcur, racc);
+                        rcur = lr;
+                        racc = 0;
+                    }
+                    racc += tr;
                 }
-            }
-            for (; k < len; k += TT) {
-                const uint32_t u = __ldcs(el_idx + e0 + k);
-                X v = (X)__ldcs(vals + e0 + k);
-                if constexpr (VLO) v += (X)__ldcs(vlo + e0 + k);
-                const uint32_t lr = u >> cb, lc = u & cmask;
-                if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;
-                sadd(yP + lr, to_fixed<X>(v * xJ[lc], scale));
-                sadd(yJ + lc, to_fixed<X>(v * xP[lr], scale));
+                if (racc != 0 && rcur < (uint32_t)nr) sadd(yP + rcur, racc);
             }
             __syncthreads();
             for (int i = threadIdx.x; i < w; i += TT) {
@@ -435,7 +485,7 @@ __global__ void k_fixed_finish(int64_t N, const double* __restrict__ diag, const
 // Calls f(p, q, v) for every stored pair (p < q, internal indices, FP64 value):
 // one CTA per panel, its dense tiles and then its leftover rows.
 template <typename V, bool VLO, typename F>
-__global__ void __launch_bounds__(TT) k_tiles_each(int64_t N, int64_t n_panels, int rb, int cb,
+__global__ void __launch_bounds__(TT) k_tiles_each(int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb,
                                                   const int64_t* __restrict__ panel_tile,
                                                   const int32_t* __restrict__ tile_win,
                                                   const int32_t* __restrict__ tile_len,
@@ -445,7 +495,7 @@ __global__ void __launch_bounds__(TT) k_tiles_each(int64_t N, int64_t n_panels, 
                                                   const uint32_t* __restrict__ el_idx, const V* __restrict__ vals,
                                                   const float* __restrict__ vlo, F f) {
     const uint32_t cmask = (1u << cb) - 1u;
-    for (int64_t P = blockIdx.x; P < n_panels; P += gridDim.x) {
+    for (int64_t P = p_lo + blockIdx.x; P < p_hi; P += gridDim.x) {
         const int64_t r0 = P << rb;
         for (int64_t t = panel_tile[P]; t < panel_tile[P + 1]; t++) {
             const int64_t c0 = (int64_t)tile_win[t] << cb, e0 = tile_off[t];
@@ -516,9 +566,10 @@ struct RowFilter {
 
 template <typename F>
 int tiles_each(risqgpu* h, F f) {
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h->n_panels, (int64_t)num_sms(h) * 8));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(h->part_p_hi - h->part_p_lo, (int64_t)num_sms(h) * 8));
 #define RQ_EACH(V, VLO, vals, lo)                                                                                   \
-    k_tiles_each<V, VLO, F><<<grid, TT, 0, h->stream>>>((int64_t)h->N, h->n_panels, h->tile_rb, h->tile_cb,         \
+    k_tiles_each<V, VLO, F><<<grid, TT, 0, h->stream>>>((int64_t)h->N, h->part_p_lo, h->part_p_hi, h->tile_rb,      \
+                                                         h->tile_cb,                                                  \
                                                          h->d_panel_tile, h->d_tile_win, h->d_tile_len,             \
                                                          h->d_tile_off, h->d_left_off, h->d_left_len, h->d_el_idx, \
                                                          vals, lo, f)
@@ -547,15 +598,19 @@ int launch_tiles(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo) 
     }
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem);
-    const int grid = (int)std::min<int64_t>(h->n_panels, (int64_t)num_sms(h) * std::max(occ, 1));
+    const int64_t own = h->part_p_hi - h->part_p_lo;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(own, (int64_t)num_sms(h) * std::max(occ, 1)));
     RQ_CUDA(h, cudaMemsetAsync(h->d_acc, 0, sizeof(long long) * N, h->stream));
     RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double), h->stream));
     k_absmax<X><<<grid_n(h, N), 256, 0, h->stream>>>(x, N, reinterpret_cast<unsigned long long*>(h->d_sig_scalars));
     k_fixed_scale<<<1, 1, 0, h->stream>>>(h->d_sig_scalars, h->h_row_abs_max, std::is_same<X, float>::value ? 100 : 1000);
-    kern<<<std::max(grid, 1), TT, smem, h->stream>>>(N, h->n_panels, h->tile_rb, h->tile_cb, h->d_panel_tile,
-                                                    h->d_tile_win, h->d_tile_len, h->d_tile_off, h->d_left_off,
-                                                    h->d_left_len, h->d_el_idx, vals, vlo, x, h->d_acc,
-                                                    h->d_sig_scalars);
+    kern<<<grid, TT, smem, h->stream>>>(N, h->part_p_lo, h->part_p_hi, h->tile_rb, h->tile_cb, h->d_panel_tile,
+                                       h->d_tile_win, h->d_tile_len, h->d_tile_off, h->d_left_off, h->d_left_len,
+                                       h->d_el_idx, vals, vlo, x, h->d_acc, h->d_sig_scalars);
+    RQ_TRY(check_launch(h, "sigma (tiles)"));
+    // with a row-block partition every rank summed its own panels: the exact integer
+    // sums are added across the ranks
+    if (h->part_n > 1) RQ_TRY(part_allreduce(h, h->d_acc, (size_t)N));
     k_fixed_finish<X><<<grid_n(h, N), 256, 0, h->stream>>>(N, h->d_diag, x, h->d_acc, h->d_sig_scalars, y);
     return check_launch(h, "sigma (tiles)");
 }
@@ -577,6 +632,18 @@ int grow(risqgpu* h, T*& p, size_t& capacity, size_t need, size_t keep) {
 
 }  // namespace
 
+int part_allreduce(risqgpu* h, void* buf_dev, size_t count) {
+    if (!h->part_reduce) {
+        h->err = "partitioned handle without a reduce function";
+        return RISQGPU_ERR_INVALID;
+    }
+    if (h->part_reduce(buf_dev, count, (void*)h->stream, h->part_user) != 0) {
+        h->err = "the caller's all-reduce failed";
+        return RISQGPU_ERR_CUDA;
+    }
+    return check_launch(h, "all-reduce");
+}
+
 int tile_shape(int64_t N, int& rb, int& cb) {
     rb = 9;   // 512 rows per panel
     cb = 12;  // 4096 columns per window
@@ -584,18 +651,23 @@ int tile_shape(int64_t N, int& rb, int& cb) {
     return ((N + ((int64_t)1 << cb) - 1) >> cb) <= MAX_BINS ? RISQGPU_OK : RISQGPU_ERR_INVALID;
 }
 
-int TileBuilder::begin(risqgpu* h_, int64_t n_panels) {
+int TileBuilder::begin(risqgpu* h_, int64_t n_panels, int64_t element_capacity) {
     h = h_;
+    el_cap = element_capacity;
     const int64_t N = (int64_t)h->N;
-    free_tiles(h);
+    // the build released the previous tiles (free_csr) and has already allocated the
+    // element arrays (d_el_idx and the values), which must survive here
+    h->tiled = false;
+    h->n_tiles = 0;
+    h->n_dense_el = 0;
     h->n_panels = n_panels;
     RQ_TRY(dalloc(h, h->d_panel_tile, (size_t)n_panels + 1));
     RQ_TRY(dalloc(h, h->d_left_off, (size_t)N));
     RQ_TRY(dalloc(h, h->d_left_len, (size_t)N));
     RQ_TRY(dalloc(h, row_abs, (size_t)N));
     RQ_TRY(dalloc(h, absmax, 1));
-    RQ_CUDA(h, cudaMemsetAsync(row_abs, 0, sizeof(float) * N, h->stream));
-    RQ_CUDA(h, cudaMemsetAsync(absmax, 0, sizeof(unsigned int), h->stream));
+    RQ_CUDA(h, cudaMemsetAsync(row_abs, 0, sizeof(unsigned long long) * N, h->stream));
+    RQ_CUDA(h, cudaMemsetAsync(absmax, 0, sizeof(unsigned long long), h->stream));
     tile_cap = 0;
     el_next = tile_next = 0;
     return RISQGPU_OK;
@@ -642,6 +714,11 @@ int TileBuilder::chunk(int64_t p_lo, int64_t p_hi, const int64_t* row_start, int
     RQ_CUDA(h, cudaMemcpyAsync(last + 3, nt64 + np - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
     RQ_TRY(sync(h, "tile offsets"));
     const int64_t el_end = last[0] + last[1], t_end = last[2] + last[3];
+    if (el_end > el_cap) {
+        h->err = "tiled layout: " + std::to_string(el_end) + " elements exceed the " + std::to_string(el_cap) +
+                 " slots counted";
+        return RISQGPU_ERR_INVALID;
+    }
     size_t c1 = tile_cap, c2 = tile_cap, c3 = tile_cap;
     RQ_TRY(grow(h, h->d_tile_win, c1, (size_t)t_end, (size_t)tile_next));
     RQ_TRY(grow(h, h->d_tile_len, c2, (size_t)t_end, (size_t)tile_next));
@@ -651,7 +728,8 @@ int TileBuilder::chunk(int64_t p_lo, int64_t p_hi, const int64_t* row_start, int
                                h->stream));
     k_tile_scatter<VIN><<<grid, TT, smem_scatter, h->stream>>>(
         N, p_lo, p_hi, rb, cb, row_start, base, row_len, cols, vin, vlo_in, el_off, t_off, ndense, h->d_left_len,
-        h->d_tile_win, h->d_tile_len, h->d_tile_off, h->d_left_off, h->d_el_idx, vout, vlo_out, row_abs);
+        h->d_tile_win, h->d_tile_len, h->d_tile_off, h->d_left_off, h->d_el_idx, vout, vlo_out, row_abs,
+        el_cap, (int64_t)tile_cap);
     RQ_TRY(check_launch(h, "tile scatter"));
     RQ_TRY(sync(h, "tile scatter"));
     el_next = el_end;
@@ -661,16 +739,19 @@ int TileBuilder::chunk(int64_t p_lo, int64_t p_hi, const int64_t* row_start, int
 
 int TileBuilder::finish() {
     const int64_t N = (int64_t)h->N;
-    RQ_CUDA(h, cudaMemcpyAsync(h->d_panel_tile + h->n_panels, &tile_next, sizeof(int64_t), cudaMemcpyHostToDevice,
+    // the tile range of this handle's last panel ends here (the panels of other ranks
+    // are not held)
+    RQ_CUDA(h, cudaMemcpyAsync(h->d_panel_tile + h->part_p_hi, &tile_next, sizeof(int64_t), cudaMemcpyHostToDevice,
                                h->stream));
-    k_max_f32<<<grid_n(h, N), 256, 0, h->stream>>>(row_abs, N, absmax);
-    unsigned int bits = 0;
-    RQ_CUDA(h, cudaMemcpyAsync(&bits, absmax, sizeof(unsigned int), cudaMemcpyDeviceToHost, h->stream));
+    // row sums of |H| over both triangles: with a partition each rank holds part of every
+    // row's sum, so the exact integer sums are added across the ranks first
+    if (h->part_n > 1) RQ_TRY(part_allreduce(h, row_abs, (size_t)N));
+    k_max_u64<<<grid_n(h, N), 256, 0, h->stream>>>(row_abs, N, absmax);
+    unsigned long long mi = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&mi, absmax, sizeof(mi), cudaMemcpyDeviceToHost, h->stream));
     RQ_TRY(sync(h, "row sums"));
-    float m;
-    std::memcpy(&m, &bits, sizeof(m));
-    // FP32 sums of |H|: a relative margin covers their rounding
-    h->h_row_abs_max = 1.01 * (double)m;
+    // each |H_pq| was rounded to a multiple of 2^-32: the margin covers that rounding
+    h->h_row_abs_max = 1.01 * ((double)mi / 4294967296.0) + 1e-6;
     h->n_tiles = tile_next;
     h->n_dense_el = 0;
     if (tile_next > 0) {

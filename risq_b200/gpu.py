@@ -223,6 +223,14 @@ class GpuHam:
         (risqgpu_set_subspace)."""
         A.check(A.lib().risqgpu_set_subspace(self._h, int(max_space), int(keep)), self._h)
 
+    def set_partition(self, rank: int, nranks: int, reduce_fn=None):
+        """Row-block partition over nranks GPUs (risqgpu_set_partition): the next
+        upper-triangle build keeps this rank's share of the row panels and sigma adds the
+        ranks' partial sums with reduce_fn (risq_b200.distributed.make_allreduce)."""
+        fn = reduce_fn if reduce_fn is not None else A.ALLREDUCE_FN()
+        A.check(A.lib().risqgpu_set_partition(self._h, int(rank), int(nranks), fn, None), self._h)
+        self._reduce_fn = fn  # the library keeps the pointer: keep the callback alive
+
     def set_memory_limit(self, nbytes: int):
         """Bound the device memory the handle may hold (0 = no bound); allocations past it
         fail with ERR_OOM (risqgpu_set_memory_limit)."""

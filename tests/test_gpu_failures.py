@@ -82,15 +82,20 @@ def test_variational_storage_fallback_under_memory_limit():
     # triangle, then columns only (the fallback chain of risqgpu_variational); a bound on the
     # handle's memory must drive it down the chain to the same wavefunction
     ints, p = H.golden_system("f2")
-    kw = dict(ncore=p["norb_core"], max_iter=20, dav_max_iter=50, precision=-1)
+    kw = dict(ncore=p["norb_core"], max_iter=20, dav_max_iter=50)
     with GpuHam(ints) as g:
-        e0, d0, c0, _, _ = g.variational(p["nup"], p["ndn"], p["eps_var"], **kw)
+        e0, d0, c0, _, _ = g.variational(p["nup"], p["ndn"], p["eps_var"], precision=-1, **kw)
         nnz_u, nnz_f = g.nnz()
         full_used, _ = g.memory_used()
     with GpuHam(ints) as g:
-        # room for the upper triangle but not both triangles of the final set
-        g.set_memory_limit(full_used - int(0.4 * nnz_f * 12))
-        e1, d1, c1, _, _ = g.variational(p["nup"], p["ndn"], p["eps_var"], **kw)
+        g.variational(p["nup"], p["ndn"], p["eps_var"], precision=_capi.FP64_UPPER, **kw)
+        upper_used, _ = g.memory_used()
+    assert upper_used < full_used
+    with GpuHam(ints) as g:
+        # half way between the two: both FP64 triangles of the final set do not fit, the
+        # upper triangle does, with room for the Davidson work space
+        g.set_memory_limit((upper_used + full_used) // 2)
+        e1, d1, c1, _, _ = g.variational(p["nup"], p["ndn"], p["eps_var"], precision=-1, **kw)
         assert g.memory_used()[0] <= g.memory_used()[1]
         nu1, nf1 = g.nnz()
     assert np.array_equal(d0, d1)

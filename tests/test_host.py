@@ -149,3 +149,45 @@ def test_replica_timing_takes_the_max_over_ranks():
     assert out[0] == 15.0 and out[1] == 15.0
     import bench
     assert bench.max_over_ranks(7.5, 1) == 7.5  # one GPU: no collective
+
+
+def _reduce_rank(rank, world, port, out):
+    import ctypes
+    import os
+
+    import numpy as np
+    import torch.distributed as dist
+
+    from risq_b200 import distributed
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        # each rank's partial fixed-point sums, wrapping in int64 as the library's do
+        part = np.arange(10, dtype=np.int64) * (rank + 1) + np.int64(2**62) * rank
+        fn = distributed.make_allreduce(host_buffers=True)
+        rc = fn(part.ctypes.data_as(ctypes.c_void_p), part.size, None, None)
+        out[rank] = (rc, part.tolist())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partition_allreduce_sums_int64_partials_across_ranks():
+    """The all-reduce a partitioned handle calls after every sigma (risqgpu_set_partition)
+    adds the ranks' int64 partial sums exactly, wrap-around included (two gloo ranks on
+    the CPU, host buffers)."""
+    import socket
+
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    procs = [ctx.Process(target=_reduce_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    want = (np.arange(10, dtype=np.int64) * 3 + np.int64(2**62)).tolist()
+    assert out[0] == (0, want) and out[1] == (0, want)
