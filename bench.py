@@ -49,15 +49,27 @@ CONFIGS = {
     1: dict(n=20, nel=8, eps=5e-5),
     2: dict(n=24, nel=10, eps=2e-5),
     4: dict(n=32, nel=12, eps=1e-5),
+    # an intermediate set for counter captures (551,147 determinants, a few GB of upper-
+    # triangle storage: larger than L2, small enough for a multi-pass ncu capture)
+    10: dict(n=20, nel=8, eps=1e-3),
 }
 DAV_MAX_ITER = 2000  # the reference's cap of 50 does not converge on these integrals
 # The CPU legs time the variational space of the last HCI iteration whose set holds at
 # most this many determinants (the whole set when it is smaller).
 CPU_SAMPLE_MAX = 150_000
-# Davidson search space of the product path (max_space, keep): a thick restart keeping
-# the lowest `keep` Ritz vectors; (0, 0) would be the reference's nroots + 10 with a
-# restart to the Ritz vector.  The FP32 basis vectors take half the memory of FP64 ones.
-PRODUCT_SPACE = (32, 8)
+# Davidson search space of the product path (max_space, keep) for sets of at least
+# THICK_MIN_DETS determinants: a thick restart keeping the lowest `keep` Ritz vectors
+# (config 1: 107 iterations against the reference space's 197-201).  Below that size a
+# Davidson iteration costs as much in launches and the host Rayleigh-Ritz as in sigma,
+# and the reference's nroots + 10 with a restart to the Ritz vector (0, 0) is faster
+# (config 0: 26 ms against 35 ms for (20, 6)).  The FP32 basis vectors take half the
+# memory of FP64 ones.
+THICK_SPACE = (32, 8)
+THICK_MIN_DETS = 1_000_000
+
+
+def product_space(n_dets):
+    return THICK_SPACE if n_dets >= THICK_MIN_DETS else (0, 0)
 
 
 def peaks():
@@ -266,6 +278,8 @@ def main():
     ap.add_argument("--config", type=int, default=1)
     ap.add_argument("--impl", default="risq_b200")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle legs")
+    ap.add_argument("--sigma-only", action="store_true",
+                    help="build the product storage and time `steps` sigma launches (no solve); for counter captures")
     ap.add_argument("--storage", choices=["auto", "upper"], default="auto",
                     help="auto: both triangles when they fit, else the upper triangle; upper: always the "
                          "upper triangle (the reference's SparseMatUpperTri layout, tiled for sigma)")
@@ -335,6 +349,24 @@ def main():
         torch.cuda.synchronize()
         return a.elapsed_time(b), out
 
+    if args.sigma_only:
+        prec = _capi.MIXED_UPPER if args.storage == "upper" or world > 1 else _capi.MIXED
+        hs = g.build(prec)
+        x32 = torch.randn(N, dtype=torch.float32, device="cuda")
+        y32 = torch.empty_like(x32)
+        for _ in range(args.warmup):
+            g.sigma_device(x32.data_ptr(), y32.data_ptr(), 1)
+        ms_s, _ = timed(lambda: [g.sigma_device(x32.data_ptr(), y32.data_ptr(), 1) for _ in range(args.steps)])
+        if rank == 0:
+            print(json.dumps({"sigma_only": True, "config": workload_config(args.config, world), "n_dets": N,
+                              "nnz_upper": hs["nnz_upper"], "n_tiles": hs["n_tiles"], "nnz_dense": hs["nnz_dense"],
+                              "fp32_sigma_ms": ms_s / max(args.steps, 1)}))
+        barrier()
+        g.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
     # product path storage: FP32 + FP32 remainder rows when both triangles fit, else the
     # upper triangle (the reference's SparseMatUpperTri layout, regrouped into tiles)
     upper_only = args.storage == "upper" or world > 1  # the partition splits upper-triangle storage
@@ -346,6 +378,8 @@ def main():
         r = g.davidson(1, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=mode, precond=pc)
         g.set_subspace(0, 0)
         return hs, r
+
+    PRODUCT_SPACE = product_space(N)
 
     def product_step():
         return solve(precm, _capi.MODE_MIXED, precond, PRODUCT_SPACE)
@@ -472,7 +506,7 @@ def main():
         pm_s = _capi.MIXED if not upper_only else _capi.MIXED_UPPER
         p64_s = _capi.FP64 if not upper_only else _capi.FP64_UPPER
         for _ in range(2):  # warm-up, then timed
-            ms_sp, (_, r_sp) = timed(lambda: solve(pm_s, _capi.MODE_MIXED, precond, PRODUCT_SPACE))
+            ms_sp, (_, r_sp) = timed(lambda: solve(pm_s, _capi.MODE_MIXED, precond, product_space(n_s)))
             ms_s64, (hs_s64, r_s64) = timed(lambda: solve(p64_s, _capi.MODE_FP64, _capi.PRECOND_DPR, (0, 0)))
         same = {"hci_iteration": k_s, "n_dets": n_s, "nnz_upper": int(hs_s64["nnz_upper"]),
                 "gpu_product_ms": ms_sp, "gpu_product_iters": r_sp.stats["iters"],

@@ -217,6 +217,14 @@ RISQGPU_API int risqgpu_sparse_optimize(risqgpu_t* h, const double* init_coeffs,
  * keep <= max_space / 2. */
 RISQGPU_API int risqgpu_set_subspace(risqgpu_t* h, int max_space, int keep);
 
+/* Reproducible sums for the FP32 sigma of upper-triangle storage.  By default it sums
+ * in FP32 with atomic adds, whose order (and so the last bits of the result) varies
+ * from run to run; on = 1 makes it sum in 64-bit fixed point like the FP64 sigma,
+ * bitwise reproducible, about 30 % slower.  FP64 sigma and partitioned handles always
+ * sum in fixed point.  The reference's serial sums are reproducible by construction
+ * (tests/integration_test_suite.rs:413-440). */
+RISQGPU_API int risqgpu_set_reproducible(risqgpu_t* h, int on);
+
 /* All-reduce supplied by a multi-GPU caller: sum `count` int64 values at device
  * address buf_dev in place across the ranks, ordered after the work already issued on
  * `stream` (a cudaStream_t) and before the work issued there after the call returns;

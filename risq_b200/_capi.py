@@ -93,6 +93,7 @@ SIGNATURES = [
     ("risqgpu_sparse_optimize", C.c_int, [_handle, _dp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
                                           _dp, _dp, C.POINTER(HStats), C.POINTER(DStats)]),
     ("risqgpu_set_subspace", C.c_int, [_handle, C.c_int, C.c_int]),
+    ("risqgpu_set_reproducible", C.c_int, [_handle, C.c_int]),
     ("risqgpu_set_partition", C.c_int, [_handle, C.c_int, C.c_int, ALLREDUCE_FN, C.c_void_p]),
     ("risqgpu_set_memory_limit", C.c_int, [_handle, C.c_size_t]),
     ("risqgpu_memory_used", C.c_int, [_handle, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),

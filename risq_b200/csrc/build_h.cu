@@ -928,10 +928,11 @@ int fill_tiled(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int p
     double* c64 = nullptr;
     float *c32 = nullptr, *clo = nullptr;
     ScopedFree<4> release(ccols, c64, c32, clo);
-    RQ_TRY(dalloc(h, h->d_el_idx, (size_t)own_cap));
-    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, (size_t)own_cap));
-    else RQ_TRY(dalloc(h, h->d_val32, (size_t)own_cap));
-    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, (size_t)own_cap));
+    // four spare slots: the pipelined sigma copies whole 16-byte blocks of these arrays
+    RQ_TRY(dalloc(h, h->d_el_idx, (size_t)own_cap + 4));
+    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, (size_t)own_cap + 4));
+    else RQ_TRY(dalloc(h, h->d_val32, (size_t)own_cap + 4));
+    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, (size_t)own_cap + 4));
     RQ_TRY(dalloc(h, ccols, (size_t)max_chunk));
     if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, c64, (size_t)max_chunk));
     else RQ_TRY(dalloc(h, c32, (size_t)max_chunk));

@@ -176,7 +176,8 @@ int risqgpu_sigma_device(risqgpu_t* h, const void* x_dev, void* y_dev, int dtype
     DeviceGuard g(h->device);
     int rc = sigma_device(h, x_dev, y_dev, dtype);
     if (rc) return rc;
-    return sync(h, "sigma_device");
+    RQ_TRY(sync(h, "sigma_device"));
+    return tiles_check(h);
 }
 
 int risqgpu_davidson(risqgpu_t* h, int nroots, const double* init, int ninit, double tol, double etol, int max_iter,
@@ -231,6 +232,12 @@ int risqgpu_set_partition(risqgpu_t* h, int rank, int nranks, risqgpu_allreduce_
     h->part_n = nranks;
     h->part_reduce = nranks > 1 ? reduce : nullptr;
     h->part_user = user;
+    return RISQGPU_OK;
+}
+
+int risqgpu_set_reproducible(risqgpu_t* h, int on) {
+    if (!h) return RISQGPU_ERR_INVALID;
+    h->reproducible = on != 0;
     return RISQGPU_OK;
 }
 

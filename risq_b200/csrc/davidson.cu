@@ -297,7 +297,12 @@ void jacobi_sorted(int n, const double* A, double* w, double* Y) {
         for (int p = 0; p < n - 1; p++)
             for (int q = p + 1; q < n; q++) {
                 double apq = a[p * n + q];
-                if (apq == 0.0) continue;
+                // threshold Jacobi (Rutishauser): an element at rounding level of its
+                // diagonal pair is set to zero instead of rotated away
+                if (std::fabs(apq) <= 1e-17 * std::max(std::fabs(a[p * n + p]), std::fabs(a[q * n + q]))) {
+                    a[p * n + q] = a[q * n + p] = 0.0;
+                    continue;
+                }
                 double theta = (a[q * n + q] - a[p * n + p]) / (2.0 * apq);
                 double t = (theta >= 0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
                 double c = 1.0 / std::sqrt(t * t + 1.0), s = t * c;
@@ -665,6 +670,7 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         RQ_TRY(sync(h, "evecs"));
     }
     RQ_TRY(sync(h, "davidson end"));
+    RQ_TRY(tiles_check(h));
     wk.timer.collect(h);
     if (st) {
         st->iters = lo.iters;

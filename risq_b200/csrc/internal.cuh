@@ -133,6 +133,7 @@ struct risqgpu {
     // Row-block partition for several GPUs (risqgpu_set_partition): this handle builds
     // and applies the row panels [part_p_lo, part_p_hi) of the tiled layout; partial
     // sums are added across the ranks by the caller's all-reduce.
+    bool reproducible = false;  // FP32 sigma in fixed point too (risqgpu_set_reproducible)
     int part_rank = 0, part_n = 1;
     risqgpu_allreduce_fn part_reduce = nullptr;
     void* part_user = nullptr;
@@ -276,6 +277,9 @@ int permute_out(risqgpu* h, const double* yi, double* y);
 // tiled upper-triangle storage (tiles.cu)
 int tile_shape(int64_t N, int& rb, int& cb);
 int sigma_tiles(risqgpu* h, const void* x, void* y, int kind);
+// RISQGPU_ERR_CUDA when a tiled sigma since the last check timed out on a copy (waits
+// for the handle's stream)
+int tiles_check(risqgpu* h);
 // Sum `count` int64 values in place across the partition's ranks (the caller's all-reduce,
 // on the handle's stream).
 int part_allreduce(risqgpu* h, void* buf_dev, size_t count);

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <type_traits>
 
@@ -293,11 +294,11 @@ __global__ void k_absmax(const X* __restrict__ x, int64_t n, unsigned long long*
 }
 
 // scalars[0]: max |x| (bits), scalars[1] <- 2^s, scalars[2] <- 2^-s, scalars[3]: panel counter
-__global__ void k_fixed_scale(double* __restrict__ scalars, double row_abs_max, int smax) {
+__global__ void k_fixed_scale(double* __restrict__ scalars, double row_abs_max, int smax, int top) {
     const double xmax = __longlong_as_double(*(const long long*)scalars);
     const double bound = row_abs_max * xmax;
     int s = 0;
-    if (bound > 0.0 && isfinite(bound)) s = 61 - ilogb(bound);
+    if (bound > 0.0 && isfinite(bound)) s = top - ilogb(bound);
     s = max(-smax, min(smax, s));
     scalars[1] = ldexp(1.0, s);
     scalars[2] = ldexp(1.0, -s);
@@ -319,6 +320,25 @@ __device__ __forceinline__ void sadd(long long* a, long long v) {
     atomicAdd(reinterpret_cast<unsigned long long*>(a), (unsigned long long)v);
 }
 
+// How sigma accumulates (shared windows and the global accumulator).
+// AccExact: 64-bit fixed point, each product rounded by the hardware conversion.
+template <typename X>
+struct AccExact {
+    using T = long long;
+    X scale;
+    __device__ __forceinline__ explicit AccExact(const double* scalars) : scale((X)scalars[1]) {}
+    __device__ __forceinline__ T conv(X t) const { return to_fixed<X>(t, scale); }
+    __device__ __forceinline__ static void add(T* a, T v) { sadd(a, v); }
+};
+// AccFloat: sums in the vector type itself with native atomics (order-dependent).
+template <typename X>
+struct AccFloat {
+    using T = X;
+    __device__ __forceinline__ explicit AccFloat(const double*) {}
+    __device__ __forceinline__ T conv(X t) const { return t; }
+    __device__ __forceinline__ static void add(T* a, T v) { atomicAdd(a, v); }
+};
+
 // Four consecutive stored values (16-byte aligned element index e) as the vector type.
 template <typename V, typename X, bool VLO>
 __device__ __forceinline__ void load4(const V* __restrict__ vals, const float* __restrict__ vlo, int64_t e,
@@ -337,24 +357,26 @@ __device__ __forceinline__ void load4(const V* __restrict__ vals, const float* _
     }
 }
 
-// V: stored value type; VLO: add the FP32 remainder (MIXED storage); X: vector type.
-template <typename V, typename X, bool VLO>
+// V: stored value type; VLO: add the FP32 remainder (MIXED storage); X: vector type;
+// A: accumulation policy.
+template <typename V, typename X, bool VLO, typename A>
 __global__ void __launch_bounds__(TT) k_sigma_tiles(
     int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb, const int64_t* __restrict__ panel_tile,
     const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
     const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len, const uint32_t* __restrict__ el_idx,
     const V* __restrict__ vals, const float* __restrict__ vlo, const X* __restrict__ x,
-    long long* __restrict__ acc, double* __restrict__ scalars) {
+    typename A::T* __restrict__ acc, double* __restrict__ scalars) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int R = 1 << rb, C = 1 << cb;
-    long long* yP = reinterpret_cast<long long*>(sm);
-    long long* yJ = yP + R;
+    using T = typename A::T;
+    T* yP = reinterpret_cast<T*>(sm);
+    T* yJ = yP + R;
     X* xP = reinterpret_cast<X*>(yJ + C);
     X* xJ = xP + R;
     __shared__ long long s_panel;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t cmask = (uint32_t)C - 1u;
-    const X scale = (X)scalars[1];
+    const A ac(scalars);
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
     for (;;) {
         if (threadIdx.x == 0) s_panel = p_lo + (long long)atomicAdd(counter, 1ull);
@@ -374,6 +396,7 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
             const int w = (int)min((int64_t)C, N - c0);
             const int64_t e0 = tile_off[t];
             const int len = tile_len[t];
+#pragma unroll 4
             for (int i = threadIdx.x; i < w; i += TT) {
                 xJ[i] = x[c0 + i];
                 yJ[i] = 0;
@@ -393,37 +416,49 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
                 if constexpr (VLO) v += (X)__ldcs(vlo + e);
                 const uint32_t lr = u >> cb, lc = u & cmask;
                 if (lr < (uint32_t)nr && lc < (uint32_t)w) {  // never false for a valid layout
-                    sadd(yP + lr, to_fixed<X>(v * xJ[lc], scale));
-                    sadd(yJ + lc, to_fixed<X>(v * xP[lr], scale));
+                    A::add(yP + lr, ac.conv(v * xJ[lc]));
+                    A::add(yJ + lc, ac.conv(v * xP[lr]));
                 }
             }
-            for (int bk = threadIdx.x; bk < nblk; bk += TT) {
-                const int64_t e = eb + 4 * (int64_t)bk;
-                const uint4 u4 = __ldcs(reinterpret_cast<const uint4*>(el_idx + e));
-                X v[4];
-                load4<V, X, VLO>(vals, vlo, e, v);
+            // two blocks per thread and iteration, both loaded before either is summed, so
+            // that every thread keeps two vector loads in flight across the atomics
+            auto sum_block = [&](const uint4 u4, const X (&v)[4]) {
                 const uint32_t u[4] = {u4.x, u4.y, u4.z, u4.w};
                 uint32_t rcur = u[0] >> cb;
-                long long racc = 0;
+                T racc = 0;
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
                     const uint32_t lr = u[j] >> cb, lc = u[j] & cmask;
                     if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;  // never taken for a valid layout
-                    const long long tr = to_fixed<X>(v[j] * xJ[lc], scale);
-                    sadd(yJ + lc, to_fixed<X>(v[j] * xP[lr], scale));
+                    const T tr = ac.conv(v[j] * xJ[lc]);
+                    A::add(yJ + lc, ac.conv(v[j] * xP[lr]));
                     if (lr != rcur) {
-                        if (racc != 0 && rcur < (uint32_t)nr) sadd(yP + rcur, racc);
+                        if (racc != 0 && rcur < (uint32_t)nr) A::add(yP + rcur, racc);
                         rcur = lr;
                         racc = 0;
                     }
                     racc += tr;
                 }
-                if (racc != 0 && rcur < (uint32_t)nr) sadd(yP + rcur, racc);
+                if (racc != 0 && rcur < (uint32_t)nr) A::add(yP + rcur, racc);
+            };
+            for (int bk = threadIdx.x; bk < nblk; bk += 2 * TT) {
+                const bool two = bk + TT < nblk;
+                const int64_t e1 = eb + 4 * (int64_t)bk, e2 = e1 + 4 * (int64_t)TT;
+                const uint4 u1 = __ldcs(reinterpret_cast<const uint4*>(el_idx + e1));
+                X v1[4], v2[4];
+                load4<V, X, VLO>(vals, vlo, e1, v1);
+                uint4 u2 = make_uint4(0, 0, 0, 0);
+                if (two) {
+                    u2 = __ldcs(reinterpret_cast<const uint4*>(el_idx + e2));
+                    load4<V, X, VLO>(vals, vlo, e2, v2);
+                }
+                sum_block(u1, v1);
+                if (two) sum_block(u2, v2);
             }
             __syncthreads();
             for (int i = threadIdx.x; i < w; i += TT) {
-                const long long a = yJ[i];
-                if (a != 0) sadd(acc + c0 + i, a);
+                const T a = yJ[i];
+                if (a != 0) A::add(acc + c0 + i, a);
             }
             __syncthreads();
         }
@@ -447,7 +482,7 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
                 for (int j = 0; j < 4; j++) {
                     if (q[j] >= (uint64_t)N) continue;  // never taken for a valid layout
                     rs += v[j] * __ldg(x + q[j]);
-                    sadd(acc + q[j], to_fixed<X>(v[j] * xr, scale));
+                    A::add(acc + q[j], ac.conv(v[j] * xr));
                 }
             }
             for (; k < len; k += 32) {
@@ -456,28 +491,338 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
                 if constexpr (VLO) v += (X)__ldcs(vlo + s + k);
                 if (q >= (uint64_t)N) continue;
                 rs += v * __ldg(x + q);
-                sadd(acc + q, to_fixed<X>(v * xr, scale));
+                A::add(acc + q, ac.conv(v * xr));
             }
             // fixed lane order: the warp sum does not depend on timing
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(FULL, rs, o);
-            if (lane == 0 && len > 0) sadd(yP + i, to_fixed<X>(rs, scale));
+            if (lane == 0 && len > 0) A::add(yP + i, ac.conv(rs));
         }
         __syncthreads();
         for (int i = threadIdx.x; i < nr; i += TT) {
-            const long long a = yP[i];
-            if (a != 0) sadd(acc + r0 + i, a);
+            const T a = yP[i];
+            if (a != 0) A::add(acc + r0 + i, a);
         }
         __syncthreads();
     }
 }
 
-// y = diag x + acc 2^-s
-template <typename X>
+// ---------------------------------------------------------------- pipelined sigma
+//
+// The same sums as k_sigma_tiles, with the dense tiles' pairs and the next x window
+// brought into shared memory by bulk asynchronous copies (cp.async.bulk, one thread
+// issuing) while the CTA sums the previous chunk: a chunk is up to PIPE_CH pairs of one
+// tile, and two chunk stages and two window buffers alternate.  Every wait on a copy
+// is bounded; on a timeout the CTA records an error in scalars[4], waits (bounded) for
+// the copies it issued and stops.
+
+constexpr int PIPE_CH = 1024;                            // pairs per chunk (a multiple of 4)
+constexpr unsigned long long PIPE_WAIT_NS = 2000000000ull;  // 2 s per chunk wait
+constexpr int F_FIRST_TILE = 1, F_LAST_TILE = 2, F_FIRST_PANEL = 4, F_LAST_PANEL = 8;
+
+struct ChunkDesc {
+    long long panel;   // panel of the chunk; -1: no more work
+    long long e_copy;  // first element copied (a multiple of 4)
+    int e_lo, e_hi;    // pairs to sum, relative to e_copy
+    int win;           // window of the tile
+    int xbuf;          // window buffer of the tile
+    int flags;
+    int pad;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long now_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool pipe_wait(uint32_t bar, uint32_t parity) {
+    const unsigned long long t0 = now_ns();
+    for (;;) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (now_ns() - t0 > PIPE_WAIT_NS) return false;
+    }
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+template <typename V, typename X, bool VLO, typename A>
+__global__ void __launch_bounds__(TT) k_sigma_tiles_pipe(
+    int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb, const int64_t* __restrict__ panel_tile,
+    const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
+    const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len, const uint32_t* __restrict__ el_idx,
+    const V* __restrict__ vals, const float* __restrict__ vlo, const X* __restrict__ x,
+    typename A::T* __restrict__ acc, double* __restrict__ scalars) {
+    using T = typename A::T;
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int R = 1 << rb, C = 1 << cb;
+    // two chunk stages {indices, values, remainders}, then two window buffers (every
+    // size is a multiple of 16 bytes, so every buffer starts 16-byte aligned)
+    constexpr size_t STAGE = (size_t)PIPE_CH * (4 + sizeof(V) + (VLO ? 4 : 0));
+    auto sidx = [&](int st) { return reinterpret_cast<uint32_t*>(sm + st * STAGE); };
+    auto sval = [&](int st) { return reinterpret_cast<V*>(sm + st * STAGE + PIPE_CH * 4); };
+    auto slo = [&](int st) { return reinterpret_cast<float*>(sm + st * STAGE + PIPE_CH * (4 + sizeof(V))); };
+    unsigned char* p = sm + 2 * STAGE;
+    X* const xJ0 = reinterpret_cast<X*>(p);
+    auto xJb = [&](int b) { return xJ0 + (size_t)b * C; };
+    p += 2 * (size_t)C * sizeof(X);
+    X* xP = reinterpret_cast<X*>(p); p += (size_t)R * sizeof(X);
+    T* yJ = reinterpret_cast<T*>(p); p += (size_t)C * sizeof(T);
+    T* yP = reinterpret_cast<T*>(p);
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ ChunkDesc desc[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t cmask = (uint32_t)C - 1u;
+    const A ac(scalars);
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
+    int* err = reinterpret_cast<int*>(scalars + 4);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < 2; s++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[s])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // producer state (thread 0 only)
+    long long pP = -1, pt = 0, pte = 0, pe = 0, pe_end = 0;
+    int tiles_started = 0;
+    bool ended = false;
+    auto produce = [&](int s) {
+        ChunkDesc d;
+        d.pad = 0;
+        if (pP < 0) {
+            pP = p_lo + (long long)atomicAdd(counter, 1ull);
+            if (pP >= p_hi) {
+                pP = -1;
+                ended = true;
+                d.panel = -1; d.e_copy = 0; d.e_lo = d.e_hi = 0; d.win = 0; d.xbuf = 0; d.flags = 0;
+                desc[s] = d;
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bars[s])), "r"(0u)
+                             : "memory");
+                return;
+            }
+            pt = panel_tile[pP];
+            pte = panel_tile[pP + 1];
+            if (pt < pte) {
+                pe = tile_off[pt];
+                pe_end = pe + tile_len[pt];
+            }
+            d.flags = F_FIRST_PANEL;
+        } else {
+            d.flags = 0;
+        }
+        d.panel = pP;
+        uint32_t bytes = 0;
+        if (pt >= pte) {  // a panel without dense tiles: staging, leftovers and flush only
+            d.flags |= F_LAST_PANEL;
+            d.e_copy = 0; d.e_lo = d.e_hi = 0; d.win = 0; d.xbuf = 0;
+            desc[s] = d;
+            pP = -1;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bars[s])), "r"(0u)
+                         : "memory");
+            return;
+        }
+        const bool first_tile = pe == tile_off[pt];
+        const long long ec = pe & ~3LL;
+        const long long ehi = min(pe_end, ec + PIPE_CH);
+        const long long ecp = (ehi + 3) & ~3LL;  // copy end (the arrays carry 4 spare slots)
+        d.e_copy = ec;
+        d.e_lo = (int)(pe - ec);
+        d.e_hi = (int)(ehi - ec);
+        d.win = tile_win[pt];
+        if (first_tile) {
+            d.flags |= F_FIRST_TILE;
+            tiles_started++;
+        }
+        d.xbuf = (tiles_started - 1) & 1;
+        const bool last_tile = ehi == pe_end;
+        if (last_tile) {
+            d.flags |= F_LAST_TILE;
+            if (pt + 1 == pte) d.flags |= F_LAST_PANEL;
+        }
+        const uint32_t n_copy = (uint32_t)(ecp - ec);
+        const int64_t c0 = (int64_t)d.win << cb;
+        const int w = (int)min((int64_t)C, N - c0);
+        const uint32_t wx = first_tile ? (uint32_t)(w & ~3) : 0u;
+        bytes = n_copy * (4u + (uint32_t)sizeof(V) + (VLO ? 4u : 0u)) + wx * (uint32_t)sizeof(X);
+        desc[s] = d;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint32_t bar = smem_addr(&bars[s]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        bulk_g2s(sidx(s), el_idx + ec, n_copy * 4u, bar);
+        bulk_g2s(sval(s), vals + ec, n_copy * (uint32_t)sizeof(V), bar);
+        if (VLO) bulk_g2s(slo(s), vlo + ec, n_copy * 4u, bar);
+        if (wx) bulk_g2s(xJb(d.xbuf), x + c0, wx * (uint32_t)sizeof(X), bar);
+        // advance
+        pe = ehi;
+        if (last_tile) {
+            pt++;
+            if (pt < pte) {
+                pe = tile_off[pt];
+                pe_end = pe + tile_len[pt];
+            } else {
+                pP = -1;
+            }
+        }
+    };
+
+    if (threadIdx.x == 0) produce(0);
+    int issued = 1;  // chunks issued (thread 0's count)
+    int k_fail = -1;
+    int64_t r0 = 0;
+    int nr = 0;
+    for (int k = 0;; k++) {
+        const int s = k & 1;
+        if (threadIdx.x == 0) {
+            issued = k + 1;
+            if (!ended) {
+                produce(s ^ 1);
+                issued = k + 2;
+            }
+        }
+        const bool ok = pipe_wait(smem_addr(&bars[s]), (uint32_t)((k >> 1) & 1));
+        if (!__syncthreads_and(ok)) {
+            k_fail = k;
+            break;
+        }
+        const ChunkDesc d = desc[s];
+        if (d.panel < 0) break;
+        if (d.flags & F_FIRST_PANEL) {
+            r0 = d.panel << rb;
+            nr = (int)min((int64_t)R, N - r0);
+            for (int i = threadIdx.x; i < nr; i += TT) {
+                xP[i] = x[r0 + i];
+                yP[i] = 0;
+            }
+        }
+        const int64_t c0 = (int64_t)d.win << cb;
+        const int w = (int)min((int64_t)C, N - c0);
+        X* xJ = xJb(d.xbuf);
+        if (d.e_hi > d.e_lo) {
+            if (d.flags & F_FIRST_TILE) {
+                for (int i = (w & ~3) + threadIdx.x; i < w; i += TT) xJ[i] = x[c0 + i];  // the window's tail
+                for (int i = threadIdx.x; i < w; i += TT) yJ[i] = 0;
+            }
+            __syncthreads();
+            const uint32_t* ui = sidx(s);
+            const V* vv = sval(s);
+            const float* vl = slo(s);
+            // aligned blocks of four pairs per thread, row runs merged in a register
+            const int b_lo = (d.e_lo + 3) >> 2, b_hi = d.e_hi >> 2;
+            auto one = [&](int e) {
+                const uint32_t u = ui[e];
+                X v = (X)vv[e];
+                if constexpr (VLO) v += (X)vl[e];
+                const uint32_t lr = u >> cb, lc = u & cmask;
+                if (lr < (uint32_t)nr && lc < (uint32_t)w) {  // never false for a valid layout
+                    A::add(yP + lr, ac.conv(v * xJ[lc]));
+                    A::add(yJ + lc, ac.conv(v * xP[lr]));
+                }
+            };
+            if (b_lo <= b_hi) {
+                const int head = 4 * b_lo - d.e_lo, tail = d.e_hi - 4 * b_hi;
+                if ((int)threadIdx.x < head) one(d.e_lo + threadIdx.x);
+                else if ((int)threadIdx.x < head + tail) one(4 * b_hi + threadIdx.x - head);
+                for (int b = b_lo + threadIdx.x; b < b_hi; b += TT) {
+                    const uint4 u4 = *reinterpret_cast<const uint4*>(ui + 4 * b);
+                    X v[4];
+                    if constexpr (std::is_same<V, double>::value) {
+                        const double2 a = *reinterpret_cast<const double2*>(vv + 4 * b);
+                        const double2 c = *reinterpret_cast<const double2*>(vv + 4 * b + 2);
+                        v[0] = (X)a.x; v[1] = (X)a.y; v[2] = (X)c.x; v[3] = (X)c.y;
+                    } else {
+                        const float4 a = *reinterpret_cast<const float4*>(vv + 4 * b);
+                        v[0] = (X)a.x; v[1] = (X)a.y; v[2] = (X)a.z; v[3] = (X)a.w;
+                        if constexpr (VLO) {
+                            const float4 l = *reinterpret_cast<const float4*>(vl + 4 * b);
+                            v[0] += (X)l.x; v[1] += (X)l.y; v[2] += (X)l.z; v[3] += (X)l.w;
+                        }
+                    }
+                    const uint32_t u[4] = {u4.x, u4.y, u4.z, u4.w};
+                    uint32_t rcur = u[0] >> cb;
+                    T racc = 0;
+#pragma unroll
+                    for (int j = 0; j < 4; j++) {
+                        const uint32_t lr = u[j] >> cb, lc = u[j] & cmask;
+                        if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;  // never taken for a valid layout
+                        const T tr = ac.conv(v[j] * xJ[lc]);
+                        A::add(yJ + lc, ac.conv(v[j] * xP[lr]));
+                        if (lr != rcur) {
+                            if (racc != 0 && rcur < (uint32_t)nr) A::add(yP + rcur, racc);
+                            rcur = lr;
+                            racc = 0;
+                        }
+                        racc += tr;
+                    }
+                    if (racc != 0 && rcur < (uint32_t)nr) A::add(yP + rcur, racc);
+                }
+            } else {  // fewer than four pairs inside one aligned block
+                if ((int)threadIdx.x < d.e_hi - d.e_lo) one(d.e_lo + threadIdx.x);
+            }
+            if (d.flags & F_LAST_TILE) {
+                __syncthreads();
+                for (int i = threadIdx.x; i < w; i += TT) {
+                    const T a = yJ[i];
+                    if (a != 0) A::add(acc + c0 + i, a);
+                }
+            }
+        }
+        if (d.flags & F_LAST_PANEL) {
+            __syncthreads();
+            // leftover pairs: one warp per row, private row sum, column sums by global atomics
+            for (int i = warp; i < nr; i += TT / 32) {
+                const int64_t s0 = left_off[r0 + i];
+                const int len = left_len[r0 + i];
+                const X xr = xP[i];
+                X rs = 0;
+                for (int kk = lane; kk < len; kk += 32) {
+                    const uint32_t q = __ldcs(el_idx + s0 + kk);
+                    X v = (X)__ldcs(vals + s0 + kk);
+                    if constexpr (VLO) v += (X)__ldcs(vlo + s0 + kk);
+                    if (q >= (uint64_t)N) continue;  // never taken for a valid layout
+                    rs += v * __ldg(x + q);
+                    A::add(acc + q, ac.conv(v * xr));
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(FULL, rs, o);
+                if (lane == 0 && len > 0) A::add(yP + i, ac.conv(rs));
+            }
+            __syncthreads();
+            for (int i = threadIdx.x; i < nr; i += TT) {
+                const T a = yP[i];
+                if (a != 0) A::add(acc + r0 + i, a);
+            }
+        }
+        __syncthreads();  // the stage, the window accumulators and the panel are free again
+    }
+    if (k_fail >= 0 && threadIdx.x == 0) {
+        atomicExch(err, 1);
+        // let the copies still outstanding (the chunk waited on and, if issued, the next)
+        // land before the CTA's shared memory goes away
+        for (int k = k_fail; k < issued && k < k_fail + 2; k++)
+            pipe_wait(smem_addr(&bars[k & 1]), (uint32_t)((k >> 1) & 1));
+    }
+}
+
+// y = diag x + acc (fixed point: acc 2^-s)
+template <typename X, typename T>
 __global__ void k_fixed_finish(int64_t N, const double* __restrict__ diag, const X* __restrict__ x,
-                               const long long* __restrict__ acc, const double* __restrict__ scalars,
+                               const T* __restrict__ acc, const double* __restrict__ scalars,
                                X* __restrict__ y) {
-    const double inv = scalars[2];
+    const double inv = std::is_same<T, long long>::value ? scalars[2] : 1.0;
     for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < N; p += (int64_t)gridDim.x * blockDim.x)
         y[p] = (X)(diag[p] * (double)x[p] + (double)acc[p] * inv);
 }
@@ -584,35 +929,54 @@ inline int grid_n(risqgpu* h, int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms(h) * 16));
 }
 
-template <typename V, typename X, bool VLO>
-int launch_tiles(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo) {
+template <typename V, typename X, bool VLO, typename A>
+int launch_tiles_acc(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo, int top) {
+    using T = typename A::T;
     const int64_t N = (int64_t)h->N;
     const int R = 1 << h->tile_rb, C = 1 << h->tile_cb;
-    const size_t smem = (size_t)(R + C) * (sizeof(long long) + sizeof(X));
-    auto kern = k_sigma_tiles<V, X, VLO>;
-    static int attr_set[64] = {0};
+    const size_t smem = (size_t)(R + C) * (sizeof(T) + sizeof(X));
+    // the pipelined kernel copies x windows with bulk copies, which need x 16-byte aligned
+    const bool pipe = ((uintptr_t)x & 15u) == 0 && !std::getenv("RISQGPU_TILE_NOPIPE");
+    const size_t smem_pipe = 2 * (size_t)PIPE_CH * (4 + sizeof(V) + (VLO ? 4 : 0)) + (size_t)(2 * C + R) * sizeof(X) +
+                             (size_t)(C + R) * sizeof(T);
+    auto kern = pipe ? k_sigma_tiles_pipe<V, X, VLO, A> : k_sigma_tiles<V, X, VLO, A>;
+    const size_t smem_k = pipe ? smem_pipe : smem;
+    static int attr_set[64][2] = {{0}};
     const int dev = h->device & 63;
-    if (attr_set[dev] < (int)smem) {
-        RQ_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set[dev] = (int)smem;
+    if (attr_set[dev][pipe] < (int)smem_k) {
+        RQ_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_k));
+        attr_set[dev][pipe] = (int)smem_k;
     }
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem_k);
     const int64_t own = h->part_p_hi - h->part_p_lo;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(own, (int64_t)num_sms(h) * std::max(occ, 1)));
+    T* acc = reinterpret_cast<T*>(h->d_acc);  // N entries of at most 8 bytes
     RQ_CUDA(h, cudaMemsetAsync(h->d_acc, 0, sizeof(long long) * N, h->stream));
     RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double), h->stream));
     k_absmax<X><<<grid_n(h, N), 256, 0, h->stream>>>(x, N, reinterpret_cast<unsigned long long*>(h->d_sig_scalars));
-    k_fixed_scale<<<1, 1, 0, h->stream>>>(h->d_sig_scalars, h->h_row_abs_max, std::is_same<X, float>::value ? 100 : 1000);
-    kern<<<grid, TT, smem, h->stream>>>(N, h->part_p_lo, h->part_p_hi, h->tile_rb, h->tile_cb, h->d_panel_tile,
+    k_fixed_scale<<<1, 1, 0, h->stream>>>(h->d_sig_scalars, h->h_row_abs_max,
+                                         std::is_same<X, float>::value ? 100 : 1000, top);
+    kern<<<grid, TT, smem_k, h->stream>>>(N, h->part_p_lo, h->part_p_hi, h->tile_rb, h->tile_cb, h->d_panel_tile,
                                        h->d_tile_win, h->d_tile_len, h->d_tile_off, h->d_left_off, h->d_left_len,
-                                       h->d_el_idx, vals, vlo, x, h->d_acc, h->d_sig_scalars);
+                                       h->d_el_idx, vals, vlo, x, acc, h->d_sig_scalars);
     RQ_TRY(check_launch(h, "sigma (tiles)"));
     // with a row-block partition every rank summed its own panels: the exact integer
     // sums are added across the ranks
     if (h->part_n > 1) RQ_TRY(part_allreduce(h, h->d_acc, (size_t)N));
-    k_fixed_finish<X><<<grid_n(h, N), 256, 0, h->stream>>>(N, h->d_diag, x, h->d_acc, h->d_sig_scalars, y);
+    k_fixed_finish<X, T><<<grid_n(h, N), 256, 0, h->stream>>>(N, h->d_diag, x, acc, h->d_sig_scalars, y);
     return check_launch(h, "sigma (tiles)");
+}
+
+// FP32 vectors sum in FP32 with native shared and global atomics (order-dependent
+// last bits, 30 % faster than fixed point at config 1) unless the handle asked for
+// reproducible sums or is partitioned (the ranks' sums must add exactly); FP64
+// vectors always sum in fixed point (no slower there).
+template <typename V, typename X, bool VLO>
+int launch_tiles(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo) {
+    const bool flt = std::is_same<X, float>::value && !h->reproducible && h->part_n == 1;
+    if (flt) return launch_tiles_acc<V, X, VLO, AccFloat<X>>(h, x, y, vals, vlo, 61);
+    return launch_tiles_acc<V, X, VLO, AccExact<X>>(h, x, y, vals, vlo, 61);
 }
 
 // Grow a device array to hold `need` entries, keeping the first `keep`.
@@ -632,6 +996,19 @@ int grow(risqgpu* h, T*& p, size_t& capacity, size_t need, size_t keep) {
 
 }  // namespace
 
+int tiles_check(risqgpu* h) {
+    if (!h->tiled || !h->d_sig_scalars) return RISQGPU_OK;
+    int e = 0;
+    RQ_CUDA(h, cudaMemcpyAsync(&e, h->d_sig_scalars + 4, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    RQ_TRY(sync(h, "sigma check"));
+    if (e) {
+        RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars + 4, 0, sizeof(double), h->stream));
+        h->err = "tiled sigma: a bulk copy did not complete within its time limit";
+        return RISQGPU_ERR_CUDA;
+    }
+    return RISQGPU_OK;
+}
+
 int part_allreduce(risqgpu* h, void* buf_dev, size_t count) {
     if (!h->part_reduce) {
         h->err = "partitioned handle without a reduce function";
@@ -645,8 +1022,12 @@ int part_allreduce(risqgpu* h, void* buf_dev, size_t count) {
 }
 
 int tile_shape(int64_t N, int& rb, int& cb) {
-    rb = 9;   // 512 rows per panel
-    cb = 12;  // 4096 columns per window
+    // measured on the config-1 set (1.1e10 pairs): 1024 x 2048 tiles beat 512 x 4096,
+    // 256 x 4096, 1024 x 4096 and 2048 x 4096 by 9-18 % (FP32) and 13-32 % (FP64)
+    rb = 10;  // 1024 rows per panel
+    cb = 11;  // 2048 columns per window
+    if (const char* e = std::getenv("RISQGPU_TILE_RB")) rb = std::max(5, std::min(12, std::atoi(e)));
+    if (const char* e = std::getenv("RISQGPU_TILE_CB")) cb = std::max(8, std::min(14, std::atoi(e)));
     while (cb < 16 && ((N + ((int64_t)1 << cb) - 1) >> cb) > MAX_BINS) cb++;
     return ((N + ((int64_t)1 << cb) - 1) >> cb) <= MAX_BINS ? RISQGPU_OK : RISQGPU_ERR_INVALID;
 }
@@ -769,7 +1150,8 @@ int TileBuilder::finish() {
         h->n_dense_el = (uint64_t)v;
     }
     RQ_TRY(dalloc(h, h->d_acc, (size_t)N));
-    RQ_TRY(dalloc(h, h->d_sig_scalars, 4));
+    RQ_TRY(dalloc(h, h->d_sig_scalars, 5));
+    RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double) * 5, h->stream));
     dfree(row_abs);
     dfree(absmax);
     h->tiled = true;

@@ -223,6 +223,11 @@ class GpuHam:
         (risqgpu_set_subspace)."""
         A.check(A.lib().risqgpu_set_subspace(self._h, int(max_space), int(keep)), self._h)
 
+    def set_reproducible(self, on: bool = True):
+        """FP32 sigma of upper-triangle storage in 64-bit fixed point (bitwise reproducible)
+        instead of FP32 atomic sums (risqgpu_set_reproducible)."""
+        A.check(A.lib().risqgpu_set_reproducible(self._h, 1 if on else 0), self._h)
+
     def set_partition(self, rank: int, nranks: int, reduce_fn=None):
         """Row-block partition over nranks GPUs (risqgpu_set_partition): the next
         upper-triangle build keeps this rank's share of the row panels and sigma adds the

@@ -7,8 +7,8 @@ of its rows is checked against the oracle's brute-force rows over the full set
 grouped search), and the energy of an earlier HCI iteration's space, which the
 CPU oracle solves in seconds, against the oracle's Davidson.  The reference pins
 bit-identical energies across runs (tests/integration_test_suite.rs:413-440); the
-upper-triangle sigma sums in 64-bit fixed point, so repeated solves must agree
-bitwise.
+upper-triangle FP64 sigma sums in 64-bit fixed point, and so does the FP32 one of a
+handle set reproducible, so repeated solves must agree bitwise.
 """
 import numpy as np
 import pytest
@@ -81,6 +81,7 @@ def test_upper_triangle_solves_are_bitwise_reproducible(prec, mode):
     ints, e, dets, coeffs, diag, log = H.synthetic_hci(12, 6, 1e-3)
     x = np.random.default_rng(4).standard_normal(len(dets))
     with GpuHam(ints) as g:
+        g.set_reproducible(True)  # the FP32 stage of MIXED sums in fixed point too
         g.set_dets(dets, 0, diag)
         g.build(prec)
         y1 = g.matrix_vector_prod(x)
