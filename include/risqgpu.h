@@ -134,7 +134,8 @@ typedef struct {
     uint64_t nnz_upper;
     double energy;
     int dav_iters;
-    int dav_converged;
+    int dav_converged;        /* 1 converged, 0 not (max iterations), -1 the matrix did not fit any storage:
+                                 the stage stopped after this iteration's selection (energy NaN) */
     double ms_select, ms_build, ms_davidson;
 } risqgpu_var_iter;
 

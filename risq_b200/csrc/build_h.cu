@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 
 #include "bits.cuh"
@@ -900,23 +901,22 @@ int fill_tiled(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int p
     const size_t base_need = (size_t)own_cap * per_el + (size_t)n * 32;
     const size_t fixed = base_need + std::max((size_t)8 << 20, std::min((size_t)256 << 20, base_need / 32));
     const size_t avail = mem_available(h);
-    // chunks: the fewest whose largest chunk fits beside the tiled arrays
+    // chunks: the fewest whose largest chunk fits beside the tiled arrays; chunk k ends at
+    // the panel boundary nearest to k/K of the pairs, so the chunks hold about equal shares
     std::vector<int64_t> cuts;
     int64_t max_chunk = 0;
     const int64_t own_np = own_hi - own_lo;
     for (int64_t K = 1;; K = K < 8 ? K + 1 : K * 2) {
-        const int64_t target = (own_cap + K - 1) / K;
         cuts.assign(1, own_lo);
-        max_chunk = 0;
-        int64_t start = own_lo;
-        for (int64_t P = own_lo + 1; P <= own_hi; P++) {
-            const bool last = P == own_hi;
-            if (last || ps[P + 1] - ps[start] > target) {
-                cuts.push_back(P);
-                max_chunk = std::max(max_chunk, ps[P] - ps[start]);
-                start = P;
-            }
+        for (int64_t k = 1; k < K; k++) {
+            const int64_t goal = ps[own_lo] + (int64_t)((double)own_cap * k / K);
+            int64_t P = std::lower_bound(ps.begin() + cuts.back() + 1, ps.begin() + own_hi, goal) - ps.begin();
+            if (P > cuts.back() + 1 && goal - ps[P - 1] < ps[P] - goal) P--;
+            if (P < own_hi) cuts.push_back(P);
         }
+        if (cuts.back() != own_hi) cuts.push_back(own_hi);
+        max_chunk = 0;
+        for (size_t c = 0; c + 1 < cuts.size(); c++) max_chunk = std::max(max_chunk, ps[cuts[c + 1]] - ps[cuts[c]]);
         if (fixed + (size_t)max_chunk * per_el <= avail) break;
         if (K >= own_np) {
             h->err = "tiled upper-triangle H needs " + std::to_string((fixed + (size_t)max_chunk * per_el) >> 20) +
@@ -928,30 +928,41 @@ int fill_tiled(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int p
     double* c64 = nullptr;
     float *c32 = nullptr, *clo = nullptr;
     ScopedFree<4> release(ccols, c64, c32, clo);
-    // four spare slots: the pipelined sigma copies whole 16-byte blocks of these arrays
-    RQ_TRY(dalloc(h, h->d_el_idx, (size_t)own_cap + 4));
-    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, (size_t)own_cap + 4));
-    else RQ_TRY(dalloc(h, h->d_val32, (size_t)own_cap + 4));
-    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, (size_t)own_cap + 4));
+    RQ_TRY(dalloc(h, h->d_el_idx, (size_t)own_cap));
+    if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, h->d_val64, (size_t)own_cap));
+    else RQ_TRY(dalloc(h, h->d_val32, (size_t)own_cap));
+    if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, h->d_val_lo, (size_t)own_cap));
     RQ_TRY(dalloc(h, ccols, (size_t)max_chunk));
     if (precision == RISQGPU_FP64) RQ_TRY(dalloc(h, c64, (size_t)max_chunk));
     else RQ_TRY(dalloc(h, c32, (size_t)max_chunk));
     if (precision == RISQGPU_MIXED) RQ_TRY(dalloc(h, clo, (size_t)max_chunk));
     TileBuilder tb;
     RQ_TRY(tb.begin(h, np, own_cap));
+    const bool verbose = std::getenv("RISQGPU_VERBOSE") != nullptr;
+    if (verbose)
+        std::fprintf(stderr, "[risqgpu] tiled build: %zu chunks, largest %lld pairs, %zu MiB available\n",
+                     cuts.size() - 1, (long long)max_chunk, avail >> 20);
     for (size_t c = 0; c + 1 < cuts.size(); c++) {
+        const auto tc0 = std::chrono::steady_clock::now();
         const int64_t p_lo = cuts[c], p_hi = cuts[c + 1];
         const int64_t r_lo = p_lo << rb, r_hi = std::min(n, p_hi << rb);
         const int64_t base = ps[p_lo];
         RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
         RQ_TRY(launch_fill<W>(h, v, I, thr, 1, precision, counter, blocks, threads, ccols, c64, c32, clo, r_lo, r_hi,
                               base));
+        if (verbose) RQ_TRY(sync(h, "fill"));
+        const auto tc1 = std::chrono::steady_clock::now();
         if (precision == RISQGPU_FP64)
             RQ_TRY(tb.chunk<double>(p_lo, p_hi, h->d_row_start, base, h->d_row_len, ccols, c64, nullptr, h->d_val64,
                                     nullptr));
         else
             RQ_TRY(tb.chunk<float>(p_lo, p_hi, h->d_row_start, base, h->d_row_len, ccols, c32, clo, h->d_val32,
                                    h->d_val_lo));
+        if (verbose)
+            std::fprintf(stderr, "[risqgpu]   chunk %zu: panels %lld..%lld fill %.1f ms, regroup %.1f ms\n", c,
+                         (long long)p_lo, (long long)p_hi,
+                         std::chrono::duration<double, std::milli>(tc1 - tc0).count(),
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc1).count());
     }
     RQ_TRY(tb.finish());
     // every stored element went into the tiles exactly once

@@ -176,8 +176,7 @@ int risqgpu_sigma_device(risqgpu_t* h, const void* x_dev, void* y_dev, int dtype
     DeviceGuard g(h->device);
     int rc = sigma_device(h, x_dev, y_dev, dtype);
     if (rc) return rc;
-    RQ_TRY(sync(h, "sigma_device"));
-    return tiles_check(h);
+    return sync(h, "sigma_device");
 }
 
 int risqgpu_davidson(risqgpu_t* h, int nroots, const double* init, int ninit, double tol, double etol, int max_iter,

@@ -670,7 +670,6 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
         RQ_TRY(sync(h, "evecs"));
     }
     RQ_TRY(sync(h, "davidson end"));
-    RQ_TRY(tiles_check(h));
     wk.timer.collect(h);
     if (st) {
         st->iters = lo.iters;

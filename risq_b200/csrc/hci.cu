@@ -277,7 +277,14 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
                 RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, 0, h->wf_diag.data()));
                 rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
             }
-            RQ_TRY(rc);
+            if (rc != RISQGPU_OK) {
+                // the space outgrew every storage mode: log the selection that got that far
+                rec.n_dets = N;
+                rec.energy = NAN;
+                rec.dav_converged = -1;
+                h->var_log.push_back(rec);
+                return rc;
+            }
             n_stored = N;
         }
         auto t2 = clk::now();

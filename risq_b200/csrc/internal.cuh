@@ -277,9 +277,6 @@ int permute_out(risqgpu* h, const double* yi, double* y);
 // tiled upper-triangle storage (tiles.cu)
 int tile_shape(int64_t N, int& rb, int& cb);
 int sigma_tiles(risqgpu* h, const void* x, void* y, int kind);
-// RISQGPU_ERR_CUDA when a tiled sigma since the last check timed out on a copy (waits
-// for the handle's stream)
-int tiles_check(risqgpu* h);
 // Sum `count` int64 values in place across the partition's ranks (the caller's all-reduce,
 // on the handle's stream).
 int part_allreduce(risqgpu* h, void* buf_dev, size_t count);

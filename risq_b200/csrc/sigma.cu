@@ -262,8 +262,7 @@ int sigma_host(risqgpu* h, const double* x, double* y, int nvec) {
         RQ_TRY(permute_out(h, dyi, dx));
         RQ_CUDA(h, cudaMemcpyAsync(y + (size_t)c * n, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
     }
-    RQ_TRY(sync(h, "sigma_host"));
-    return tiles_check(h);
+    return sync(h, "sigma_host");
 }
 
 int self_energy_impl(risqgpu* h, double energy, double gmin, double* out) {

@@ -507,316 +507,6 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
     }
 }
 
-// ---------------------------------------------------------------- pipelined sigma
-//
-// The same sums as k_sigma_tiles, with the dense tiles' pairs and the next x window
-// brought into shared memory by bulk asynchronous copies (cp.async.bulk, one thread
-// issuing) while the CTA sums the previous chunk: a chunk is up to PIPE_CH pairs of one
-// tile, and two chunk stages and two window buffers alternate.  Every wait on a copy
-// is bounded; on a timeout the CTA records an error in scalars[4], waits (bounded) for
-// the copies it issued and stops.
-
-constexpr int PIPE_CH = 1024;                            // pairs per chunk (a multiple of 4)
-constexpr unsigned long long PIPE_WAIT_NS = 2000000000ull;  // 2 s per chunk wait
-constexpr int F_FIRST_TILE = 1, F_LAST_TILE = 2, F_FIRST_PANEL = 4, F_LAST_PANEL = 8;
-
-struct ChunkDesc {
-    long long panel;   // panel of the chunk; -1: no more work
-    long long e_copy;  // first element copied (a multiple of 4)
-    int e_lo, e_hi;    // pairs to sum, relative to e_copy
-    int win;           // window of the tile
-    int xbuf;          // window buffer of the tile
-    int flags;
-    int pad;
-};
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ unsigned long long now_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ bool pipe_wait(uint32_t bar, uint32_t parity) {
-    const unsigned long long t0 = now_ns();
-    for (;;) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-        if (now_ns() - t0 > PIPE_WAIT_NS) return false;
-    }
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-template <typename V, typename X, bool VLO, typename A>
-__global__ void __launch_bounds__(TT) k_sigma_tiles_pipe(
-    int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb, const int64_t* __restrict__ panel_tile,
-    const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
-    const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len, const uint32_t* __restrict__ el_idx,
-    const V* __restrict__ vals, const float* __restrict__ vlo, const X* __restrict__ x,
-    typename A::T* __restrict__ acc, double* __restrict__ scalars) {
-    using T = typename A::T;
-    extern __shared__ __align__(16) unsigned char sm[];
-    const int R = 1 << rb, C = 1 << cb;
-    // two chunk stages {indices, values, remainders}, then two window buffers (every
-    // size is a multiple of 16 bytes, so every buffer starts 16-byte aligned)
-    constexpr size_t STAGE = (size_t)PIPE_CH * (4 + sizeof(V) + (VLO ? 4 : 0));
-    auto sidx = [&](int st) { return reinterpret_cast<uint32_t*>(sm + st * STAGE); };
-    auto sval = [&](int st) { return reinterpret_cast<V*>(sm + st * STAGE + PIPE_CH * 4); };
-    auto slo = [&](int st) { return reinterpret_cast<float*>(sm + st * STAGE + PIPE_CH * (4 + sizeof(V))); };
-    unsigned char* p = sm + 2 * STAGE;
-    X* const xJ0 = reinterpret_cast<X*>(p);
-    auto xJb = [&](int b) { return xJ0 + (size_t)b * C; };
-    p += 2 * (size_t)C * sizeof(X);
-    X* xP = reinterpret_cast<X*>(p); p += (size_t)R * sizeof(X);
-    T* yJ = reinterpret_cast<T*>(p); p += (size_t)C * sizeof(T);
-    T* yP = reinterpret_cast<T*>(p);
-    __shared__ __align__(8) uint64_t bars[2];
-    __shared__ ChunkDesc desc[2];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t cmask = (uint32_t)C - 1u;
-    const A ac(scalars);
-    unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
-    int* err = reinterpret_cast<int*>(scalars + 4);
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < 2; s++) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&bars[s])));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-
-    // producer state (thread 0 only)
-    long long pP = -1, pt = 0, pte = 0, pe = 0, pe_end = 0;
-    int tiles_started = 0;
-    bool ended = false;
-    auto produce = [&](int s) {
-        ChunkDesc d;
-        d.pad = 0;
-        if (pP < 0) {
-            pP = p_lo + (long long)atomicAdd(counter, 1ull);
-            if (pP >= p_hi) {
-                pP = -1;
-                ended = true;
-                d.panel = -1; d.e_copy = 0; d.e_lo = d.e_hi = 0; d.win = 0; d.xbuf = 0; d.flags = 0;
-                desc[s] = d;
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bars[s])), "r"(0u)
-                             : "memory");
-                return;
-            }
-            pt = panel_tile[pP];
-            pte = panel_tile[pP + 1];
-            if (pt < pte) {
-                pe = tile_off[pt];
-                pe_end = pe + tile_len[pt];
-            }
-            d.flags = F_FIRST_PANEL;
-        } else {
-            d.flags = 0;
-        }
-        d.panel = pP;
-        uint32_t bytes = 0;
-        if (pt >= pte) {  // a panel without dense tiles: staging, leftovers and flush only
-            d.flags |= F_LAST_PANEL;
-            d.e_copy = 0; d.e_lo = d.e_hi = 0; d.win = 0; d.xbuf = 0;
-            desc[s] = d;
-            pP = -1;
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&bars[s])), "r"(0u)
-                         : "memory");
-            return;
-        }
-        const bool first_tile = pe == tile_off[pt];
-        const long long ec = pe & ~3LL;
-        const long long ehi = min(pe_end, ec + PIPE_CH);
-        const long long ecp = (ehi + 3) & ~3LL;  // copy end (the arrays carry 4 spare slots)
-        d.e_copy = ec;
-        d.e_lo = (int)(pe - ec);
-        d.e_hi = (int)(ehi - ec);
-        d.win = tile_win[pt];
-        if (first_tile) {
-            d.flags |= F_FIRST_TILE;
-            tiles_started++;
-        }
-        d.xbuf = (tiles_started - 1) & 1;
-        const bool last_tile = ehi == pe_end;
-        if (last_tile) {
-            d.flags |= F_LAST_TILE;
-            if (pt + 1 == pte) d.flags |= F_LAST_PANEL;
-        }
-        const uint32_t n_copy = (uint32_t)(ecp - ec);
-        const int64_t c0 = (int64_t)d.win << cb;
-        const int w = (int)min((int64_t)C, N - c0);
-        const uint32_t wx = first_tile ? (uint32_t)(w & ~3) : 0u;
-        bytes = n_copy * (4u + (uint32_t)sizeof(V) + (VLO ? 4u : 0u)) + wx * (uint32_t)sizeof(X);
-        desc[s] = d;
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const uint32_t bar = smem_addr(&bars[s]);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-        bulk_g2s(sidx(s), el_idx + ec, n_copy * 4u, bar);
-        bulk_g2s(sval(s), vals + ec, n_copy * (uint32_t)sizeof(V), bar);
-        if (VLO) bulk_g2s(slo(s), vlo + ec, n_copy * 4u, bar);
-        if (wx) bulk_g2s(xJb(d.xbuf), x + c0, wx * (uint32_t)sizeof(X), bar);
-        // advance
-        pe = ehi;
-        if (last_tile) {
-            pt++;
-            if (pt < pte) {
-                pe = tile_off[pt];
-                pe_end = pe + tile_len[pt];
-            } else {
-                pP = -1;
-            }
-        }
-    };
-
-    if (threadIdx.x == 0) produce(0);
-    int issued = 1;  // chunks issued (thread 0's count)
-    int k_fail = -1;
-    int64_t r0 = 0;
-    int nr = 0;
-    for (int k = 0;; k++) {
-        const int s = k & 1;
-        if (threadIdx.x == 0) {
-            issued = k + 1;
-            if (!ended) {
-                produce(s ^ 1);
-                issued = k + 2;
-            }
-        }
-        const bool ok = pipe_wait(smem_addr(&bars[s]), (uint32_t)((k >> 1) & 1));
-        if (!__syncthreads_and(ok)) {
-            k_fail = k;
-            break;
-        }
-        const ChunkDesc d = desc[s];
-        if (d.panel < 0) break;
-        if (d.flags & F_FIRST_PANEL) {
-            r0 = d.panel << rb;
-            nr = (int)min((int64_t)R, N - r0);
-            for (int i = threadIdx.x; i < nr; i += TT) {
-                xP[i] = x[r0 + i];
-                yP[i] = 0;
-            }
-        }
-        const int64_t c0 = (int64_t)d.win << cb;
-        const int w = (int)min((int64_t)C, N - c0);
-        X* xJ = xJb(d.xbuf);
-        if (d.e_hi > d.e_lo) {
-            if (d.flags & F_FIRST_TILE) {
-                for (int i = (w & ~3) + threadIdx.x; i < w; i += TT) xJ[i] = x[c0 + i];  // the window's tail
-                for (int i = threadIdx.x; i < w; i += TT) yJ[i] = 0;
-            }
-            __syncthreads();
-            const uint32_t* ui = sidx(s);
-            const V* vv = sval(s);
-            const float* vl = slo(s);
-            // aligned blocks of four pairs per thread, row runs merged in a register
-            const int b_lo = (d.e_lo + 3) >> 2, b_hi = d.e_hi >> 2;
-            auto one = [&](int e) {
-                const uint32_t u = ui[e];
-                X v = (X)vv[e];
-                if constexpr (VLO) v += (X)vl[e];
-                const uint32_t lr = u >> cb, lc = u & cmask;
-                if (lr < (uint32_t)nr && lc < (uint32_t)w) {  // never false for a valid layout
-                    A::add(yP + lr, ac.conv(v * xJ[lc]));
-                    A::add(yJ + lc, ac.conv(v * xP[lr]));
-                }
-            };
-            if (b_lo <= b_hi) {
-                const int head = 4 * b_lo - d.e_lo, tail = d.e_hi - 4 * b_hi;
-                if ((int)threadIdx.x < head) one(d.e_lo + threadIdx.x);
-                else if ((int)threadIdx.x < head + tail) one(4 * b_hi + threadIdx.x - head);
-                for (int b = b_lo + threadIdx.x; b < b_hi; b += TT) {
-                    const uint4 u4 = *reinterpret_cast<const uint4*>(ui + 4 * b);
-                    X v[4];
-                    if constexpr (std::is_same<V, double>::value) {
-                        const double2 a = *reinterpret_cast<const double2*>(vv + 4 * b);
-                        const double2 c = *reinterpret_cast<const double2*>(vv + 4 * b + 2);
-                        v[0] = (X)a.x; v[1] = (X)a.y; v[2] = (X)c.x; v[3] = (X)c.y;
-                    } else {
-                        const float4 a = *reinterpret_cast<const float4*>(vv + 4 * b);
-                        v[0] = (X)a.x; v[1] = (X)a.y; v[2] = (X)a.z; v[3] = (X)a.w;
-                        if constexpr (VLO) {
-                            const float4 l = *reinterpret_cast<const float4*>(vl + 4 * b);
-                            v[0] += (X)l.x; v[1] += (X)l.y; v[2] += (X)l.z; v[3] += (X)l.w;
-                        }
-                    }
-                    const uint32_t u[4] = {u4.x, u4.y, u4.z, u4.w};
-                    uint32_t rcur = u[0] >> cb;
-                    T racc = 0;
-#pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const uint32_t lr = u[j] >> cb, lc = u[j] & cmask;
-                        if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;  // never taken for a valid layout
-                        const T tr = ac.conv(v[j] * xJ[lc]);
-                        A::add(yJ + lc, ac.conv(v[j] * xP[lr]));
-                        if (lr != rcur) {
-                            if (racc != 0 && rcur < (uint32_t)nr) A::add(yP + rcur, racc);
-                            rcur = lr;
-                            racc = 0;
-                        }
-                        racc += tr;
-                    }
-                    if (racc != 0 && rcur < (uint32_t)nr) A::add(yP + rcur, racc);
-                }
-            } else {  // fewer than four pairs inside one aligned block
-                if ((int)threadIdx.x < d.e_hi - d.e_lo) one(d.e_lo + threadIdx.x);
-            }
-            if (d.flags & F_LAST_TILE) {
-                __syncthreads();
-                for (int i = threadIdx.x; i < w; i += TT) {
-                    const T a = yJ[i];
-                    if (a != 0) A::add(acc + c0 + i, a);
-                }
-            }
-        }
-        if (d.flags & F_LAST_PANEL) {
-            __syncthreads();
-            // leftover pairs: one warp per row, private row sum, column sums by global atomics
-            for (int i = warp; i < nr; i += TT / 32) {
-                const int64_t s0 = left_off[r0 + i];
-                const int len = left_len[r0 + i];
-                const X xr = xP[i];
-                X rs = 0;
-                for (int kk = lane; kk < len; kk += 32) {
-                    const uint32_t q = __ldcs(el_idx + s0 + kk);
-                    X v = (X)__ldcs(vals + s0 + kk);
-                    if constexpr (VLO) v += (X)__ldcs(vlo + s0 + kk);
-                    if (q >= (uint64_t)N) continue;  // never taken for a valid layout
-                    rs += v * __ldg(x + q);
-                    A::add(acc + q, ac.conv(v * xr));
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(FULL, rs, o);
-                if (lane == 0 && len > 0) A::add(yP + i, ac.conv(rs));
-            }
-            __syncthreads();
-            for (int i = threadIdx.x; i < nr; i += TT) {
-                const T a = yP[i];
-                if (a != 0) A::add(acc + r0 + i, a);
-            }
-        }
-        __syncthreads();  // the stage, the window accumulators and the panel are free again
-    }
-    if (k_fail >= 0 && threadIdx.x == 0) {
-        atomicExch(err, 1);
-        // let the copies still outstanding (the chunk waited on and, if issued, the next)
-        // land before the CTA's shared memory goes away
-        for (int k = k_fail; k < issued && k < k_fail + 2; k++)
-            pipe_wait(smem_addr(&bars[k & 1]), (uint32_t)((k >> 1) & 1));
-    }
-}
-
 // y = diag x + acc (fixed point: acc 2^-s)
 template <typename X, typename T>
 __global__ void k_fixed_finish(int64_t N, const double* __restrict__ diag, const X* __restrict__ x,
@@ -935,17 +625,13 @@ int launch_tiles_acc(risqgpu* h, const X* x, X* y, const V* vals, const float* v
     const int64_t N = (int64_t)h->N;
     const int R = 1 << h->tile_rb, C = 1 << h->tile_cb;
     const size_t smem = (size_t)(R + C) * (sizeof(T) + sizeof(X));
-    // the pipelined kernel copies x windows with bulk copies, which need x 16-byte aligned
-    const bool pipe = ((uintptr_t)x & 15u) == 0 && !std::getenv("RISQGPU_TILE_NOPIPE");
-    const size_t smem_pipe = 2 * (size_t)PIPE_CH * (4 + sizeof(V) + (VLO ? 4 : 0)) + (size_t)(2 * C + R) * sizeof(X) +
-                             (size_t)(C + R) * sizeof(T);
-    auto kern = pipe ? k_sigma_tiles_pipe<V, X, VLO, A> : k_sigma_tiles<V, X, VLO, A>;
-    const size_t smem_k = pipe ? smem_pipe : smem;
-    static int attr_set[64][2] = {{0}};
+    auto kern = k_sigma_tiles<V, X, VLO, A>;
+    const size_t smem_k = smem;
+    static int attr_set[64] = {0};
     const int dev = h->device & 63;
-    if (attr_set[dev][pipe] < (int)smem_k) {
+    if (attr_set[dev] < (int)smem_k) {
         RQ_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_k));
-        attr_set[dev][pipe] = (int)smem_k;
+        attr_set[dev] = (int)smem_k;
     }
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem_k);
@@ -996,19 +682,6 @@ int grow(risqgpu* h, T*& p, size_t& capacity, size_t need, size_t keep) {
 
 }  // namespace
 
-int tiles_check(risqgpu* h) {
-    if (!h->tiled || !h->d_sig_scalars) return RISQGPU_OK;
-    int e = 0;
-    RQ_CUDA(h, cudaMemcpyAsync(&e, h->d_sig_scalars + 4, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
-    RQ_TRY(sync(h, "sigma check"));
-    if (e) {
-        RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars + 4, 0, sizeof(double), h->stream));
-        h->err = "tiled sigma: a bulk copy did not complete within its time limit";
-        return RISQGPU_ERR_CUDA;
-    }
-    return RISQGPU_OK;
-}
-
 int part_allreduce(risqgpu* h, void* buf_dev, size_t count) {
     if (!h->part_reduce) {
         h->err = "partitioned handle without a reduce function";
@@ -1026,8 +699,6 @@ int tile_shape(int64_t N, int& rb, int& cb) {
     // 256 x 4096, 1024 x 4096 and 2048 x 4096 by 9-18 % (FP32) and 13-32 % (FP64)
     rb = 10;  // 1024 rows per panel
     cb = 11;  // 2048 columns per window
-    if (const char* e = std::getenv("RISQGPU_TILE_RB")) rb = std::max(5, std::min(12, std::atoi(e)));
-    if (const char* e = std::getenv("RISQGPU_TILE_CB")) cb = std::max(8, std::min(14, std::atoi(e)));
     while (cb < 16 && ((N + ((int64_t)1 << cb) - 1) >> cb) > MAX_BINS) cb++;
     return ((N + ((int64_t)1 << cb) - 1) >> cb) <= MAX_BINS ? RISQGPU_OK : RISQGPU_ERR_INVALID;
 }
@@ -1150,8 +821,7 @@ int TileBuilder::finish() {
         h->n_dense_el = (uint64_t)v;
     }
     RQ_TRY(dalloc(h, h->d_acc, (size_t)N));
-    RQ_TRY(dalloc(h, h->d_sig_scalars, 5));
-    RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double) * 5, h->stream));
+    RQ_TRY(dalloc(h, h->d_sig_scalars, 4));
     dfree(row_abs);
     dfree(absmax);
     h->tiled = true;
