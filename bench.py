@@ -47,13 +47,22 @@ METRIC = "time-to-E_var (≤1µHa vs FP64): mixed+learned vs plain GPU; σ GB/s;
 CONFIGS = {
     0: dict(n=12, nel=6, eps=1e-4),
     1: dict(n=20, nel=8, eps=5e-5),
-    2: dict(n=24, nel=10, eps=2e-5),
+    # n24: the first 4 HCI iterations (5,042,871 determinants, 5.6e9 upper pairs); the
+    # 5th iteration's set (42,294,108 determinants) needs 525 GB for its columns alone,
+    # and its matrix-free sigma is timed separately.  Also a 2-root leg.
+    2: dict(n=24, nel=10, eps=2e-5, hci_iters=4, two_roots=True),
     4: dict(n=32, nel=12, eps=1e-5),
     # an intermediate set for counter captures (551,147 determinants, a few GB of upper-
     # triangle storage: larger than L2, small enough for a multi-pass ncu capture)
     10: dict(n=20, nel=8, eps=1e-3),
 }
 DAV_MAX_ITER = 2000  # the reference's cap of 50 does not converge on these integrals
+# DRAM bytes (read + write) of one FP32 tiled sigma launch from one ncu capture of the
+# kernel on the n20 eps 1e-3 set (profiles/k_sigma_tiles_fp32_n20_eps1e-3.md); the
+# element stream is the traffic and grows with the stored pairs, so a launch over
+# another set is scaled by its pairs
+SIGMA32_CAPTURE = {"pairs": 334_413_323, "dram_bytes": 2_692_757_760 + 6_486_016,
+                   "set": "n20 8a8b eps_var 1e-3 seed 0 (551,147 dets)"}
 # The CPU legs time the variational space of the last HCI iteration whose set holds at
 # most this many determinants (the whole set when it is smaller).
 CPU_SAMPLE_MAX = 150_000
@@ -68,8 +77,10 @@ THICK_SPACE = (32, 8)
 THICK_MIN_DETS = 1_000_000
 
 
-def product_space(n_dets):
-    return THICK_SPACE if n_dets >= THICK_MIN_DETS else (0, 0)
+def product_space(n_dets, nroots=1):
+    """(max_space, keep) of the product path; (0, 0) is the reference's space
+    (nroots + 10, restart to the Ritz vectors)."""
+    return THICK_SPACE if n_dets >= THICK_MIN_DETS and THICK_SPACE[1] >= nroots else (0, 0)
 
 
 def peaks():
@@ -84,7 +95,8 @@ def peaks():
 def workload_config(cfg_id, world):
     """The `config` dict both arms print (the workload, not how one arm stores it)."""
     c = CONFIGS[cfg_id]
-    return {"workload": f"hci n{c['n']} {c['nel']}a{c['nel']}b eps_var {c['eps']:g} seed 0",
+    iters = f", HCI iterations 1-{c['hci_iters']}" if "hci_iters" in c else ""
+    return {"workload": f"hci n{c['n']} {c['nel']}a{c['nel']}b eps_var {c['eps']:g} seed 0{iters}",
             "step": "sparse-H build + Davidson to E_var (tol 1e-4, etol 1e-8) from the reference's default start",
             "l2": "CSR stream larger than L2 every step",
             "parallelism": "one GPU" if world == 1 else f"row blocks x{world}, all-reduce of sigma partial sums"}
@@ -180,14 +192,15 @@ def det_set(cfg_id, device, log=print):
     c = CONFIGS[cfg_id]
     ints = synthetic_integrals(c["n"], 0)
     os.makedirs(os.path.join(ROOT, "data"), exist_ok=True)
-    path = os.path.join(ROOT, "data", f"hci_n{c['n']}_{c['nel']}_{c['eps']:g}_s0.npz")
+    max_iter = c.get("hci_iters", 20)
+    path = os.path.join(ROOT, "data", f"hci_n{c['n']}_{c['nel']}_{c['eps']:g}_s0_i{max_iter}.npz")
     if os.path.exists(path):
         z = np.load(path, allow_pickle=True)
         return ints, z["dets"], z["diag"], float(z["energy"]), list(z["log"])
     t0 = time.time()
     with GpuHam(ints, device) as g:
         # precision -1: FP64 while the matrix fits, then the upper triangle, then columns only
-        e, dets, coeffs, diag, vlog = g.variational(c["nel"], c["nel"], c["eps"], max_iter=20,
+        e, dets, coeffs, diag, vlog = g.variational(c["nel"], c["nel"], c["eps"], max_iter=max_iter,
                                                     dav_max_iter=DAV_MAX_ITER, precision=-1)
     log(f"# det set config {cfg_id}: N={len(dets)} E={e:.10f} ({time.time() - t0:.1f} s)")
     for r in vlog:
@@ -237,7 +250,7 @@ def run_reference(args):
     t0 = time.perf_counter()
     hci = O.Hci(oh, cfg["nel"], cfg["nel"], cfg["eps"]).set_options(DAV_MAX_ITER, parallel=True)
     prev = None
-    for it in range(20):
+    for it in range(cfg.get("hci_iters", 20)):
         rc = hci.step_bounded(CPU_SAMPLE_MAX)
         if rc != 0:
             break
@@ -436,6 +449,23 @@ def main():
     ms_l, (_, r_l) = timed(lambda: solve(prec64, _capi.MODE_FP64, _capi.PRECOND_DPR, PRODUCT_SPACE))
     legs["fp64_product_space"] = (ms_l, r_l)
 
+    # ---- two roots (block Davidson, davidson.rs:53-79 with nroots = 2): product path
+    # against plain FP64, each root within 1 uHa ----
+    two_roots = None
+    if cfg.get("two_roots"):
+        def solve2(prec, mode, pc, space):
+            g.set_subspace(*space)
+            g.build(prec)
+            r = g.davidson(2, None, 1e-4, 1e-8, DAV_MAX_ITER, mode=mode, precond=pc)
+            g.set_subspace(0, 0)
+            return r
+        ms2m, r2m = timed(lambda: solve2(precm, _capi.MODE_MIXED, _capi.PRECOND_DPR, product_space(N, 2)))
+        ms2p, r2p = timed(lambda: solve2(prec64, _capi.MODE_FP64, _capi.PRECOND_DPR, (0, 0)))
+        two_roots = {"mixed_ms": ms2m, "mixed_iters": r2m.stats["iters"], "mixed_energies": [float(e) for e in r2m.eigenvalues],
+                     "fp64_ms": ms2p, "fp64_iters": r2p.stats["iters"], "fp64_energies": [float(e) for e in r2p.eigenvalues],
+                     "converged": bool(r2m.converged and r2p.converged),
+                     "dE_uHa": [abs(float(a) - float(b)) * 1e6 for a, b in zip(r2m.eigenvalues, r2p.eigenvalues)]}
+
     # ---- sigma roofline, FP64 (x, y in the library's internal order) ----
     nnz_u, nnz_f = g.nnz()  # this rank's pairs (all of them on one GPU)
     nnz_u_all, nnz_f_all = sum_over_ranks(nnz_u, world), sum_over_ranks(nnz_f, world)
@@ -550,7 +580,10 @@ def main():
                      "kernel": "k_spmv<FP32>" if full_m else "k_sigma_tiles<FP32>",
                      "achieved": sig32_gbs, "peak": peak, "unit": "GB/s",
                      "frac": sig32_gbs / peak, "peak_kind": peak_kind,
-                     "traffic": None,
+                     "traffic": None if full_m else
+                     SIGMA32_CAPTURE["dram_bytes"] / SIGMA32_CAPTURE["pairs"] * nnz_u,
+                     "traffic_source": None if full_m else
+                     f"ncu DRAM bytes of the same kernel on {SIGMA32_CAPTURE['set']}, scaled by stored pairs",
                      "bytes_per_launch": int(b_sig32), "ms_per_launch": t_sig32},
         "time_to_evar_ms": {"mixed_learned": ms_max, "fp64_plain": ms_plain,
                             "speedup_vs_fp64_plain": ms_plain / ms_max,
@@ -574,6 +607,7 @@ def main():
                      "mixed_ms": r_m.stats["ms_total"], "mixed_ms_sigma": r_m.stats["ms_sigma"],
                      "fp64_ms": r64.stats["ms_total"], "fp64_ms_sigma": r64.stats["ms_sigma"]},
         "same_set": same,
+        "two_roots": two_roots,
         "clocks": clk,
         "gpu_launches": launches_per_step * args.steps if launches_per_step is not None else None,
         "gpu_launches_per_step": launches_per_step,

@@ -68,12 +68,19 @@ enum risqgpu_precision {
                            (bitwise the stored FP64 values) for sets whose values do not fit */
     /* Upper triangle only (each pair once, as the reference's SparseMatUpperTri): half the
      * storage.  The pairs are regrouped into row-panel x column-window tiles whose x and
-     * y windows sigma stages in shared memory; sums are formed in 64-bit fixed point, so
-     * sigma and the solves built on it are bitwise reproducible.  Built from scratch
-     * every time (no n_stored_h reuse). */
+     * y windows sigma stages in shared memory.  The FP64 sigma sums in 64-bit fixed
+     * point, so it and the solves built on it are bitwise reproducible; the FP32 sigma
+     * sums in FP32 (order-dependent in the last bits) unless risqgpu_set_reproducible
+     * asks for fixed point too.  Built from scratch every time (no n_stored_h reuse). */
     RISQGPU_FP64_UPPER = 4,
     RISQGPU_FP32_UPPER = 5,
-    RISQGPU_MIXED_UPPER = 6
+    RISQGPU_MIXED_UPPER = 6,
+    /* Nothing stored: the FP64 sigma runs the build's connection search and evaluates
+     * every element of every row itself (both triangles, the elements a FP64 build with
+     * the same builder rule stores, bitwise), one warp per row with a private sum, so it
+     * is bitwise reproducible.  For sets whose columns do not fit; about 20x the time of
+     * a stored sigma.  No FP32 sigma, export, self energy or row-block partition. */
+    RISQGPU_MATRIX_FREE = 7
 };
 
 /* Which reference builder's rule decides the stored set (src/var/davidson.rs:55-61). */
@@ -137,6 +144,7 @@ typedef struct {
     int dav_converged;        /* 1 converged, 0 not (max iterations), -1 the matrix did not fit any storage:
                                  the stage stopped after this iteration's selection (energy NaN) */
     double ms_select, ms_build, ms_davidson;
+    int storage;              /* the iteration's H storage (RISQGPU_FP64 ... RISQGPU_MATRIX_FREE), -1 none */
 } risqgpu_var_iter;
 
 /* Library version string. */
@@ -275,7 +283,10 @@ RISQGPU_API int risqgpu_get_new_dets(risqgpu_t* h, uint64_t* dets, double* diag,
  * src/var/mod.rs:59-134) on the device: HF start, eps schedule, selection,
  * incremental H build and Davidson each iteration.  z_sym must be 1.  max_iter: HCI
  * iterations (the reference uses 20); dav_max_iter: Davidson iterations per solve (the
- * reference uses 50).  The final wavefunction stays in the handle (risqgpu_get_wf). */
+ * reference uses 50).  precision -1 stores FP64 both triangles while they fit, then
+ * falls back, as the set grows, to FP64_UPPER, COLS and MATRIX_FREE (each OOM moves
+ * one step down); otherwise the given storage every iteration.  The final
+ * wavefunction stays in the handle (risqgpu_get_wf). */
 RISQGPU_API int risqgpu_variational(risqgpu_t* h, int nup, int ndn, int ncore, int z_sym, double eps_var,
                                     int max_iter, int dav_max_iter, int precision, int mode, int precond,
                                     double* energy, uint64_t* n_dets);
@@ -296,10 +307,10 @@ RISQGPU_API int risqgpu_var_log(risqgpu_t* h, risqgpu_var_iter* out, int cap, in
  * Ordering: the call runs on the handle's stream, which by default does not wait
  * for other streams.  x_dev must therefore be complete before the call, or the
  * caller routes the handle onto the stream that produces x_dev with
- * risqgpu_set_stream.  The call returns after its own work has finished.
- * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress, with the handle's device current), so make that first
- * call before any CUDA stream capture begins.  All calls share the array, so
+ * risqgpu_set_stream.  The call synchronises the handle's stream before it returns,
+ * so it cannot be recorded into a CUDA graph by stream capture.  The first call on
+ * each device also looks up the array's device address (cudaGetSymbolAddress, with
+ * the handle's device current).  All calls share the array, so
  * calls that overlap on the GPU (other handles or threads, other streams) race;
  * the contents left by a previous call are never read. */
 RISQGPU_API int risqgpu_sigma_noalloc(risqgpu_t* h, const double* x_dev, double* y_dev);

@@ -20,7 +20,7 @@ ERR_NOT_CONVERGED = 4
 ERR_NO_DEVICE = 5
 ERR_CAPACITY = 6
 
-FP64, FP32, MIXED, COLS, FP64_UPPER, FP32_UPPER, MIXED_UPPER = 0, 1, 2, 3, 4, 5, 6
+FP64, FP32, MIXED, COLS, FP64_UPPER, FP32_UPPER, MIXED_UPPER, MATRIX_FREE = 0, 1, 2, 3, 4, 5, 6, 7
 BUILDER_AUTO, BUILDER_FAST, BUILDER_LEGACY = 0, 1, 2
 MODE_FP64, MODE_MIXED, MODE_FP32 = 0, 1, 2
 PRECOND_DPR, PRECOND_LEARNED = 0, 1
@@ -58,7 +58,7 @@ class VarIter(C.Structure):
     _fields_ = [("eps", C.c_double), ("n_dets", C.c_uint64), ("n_new", C.c_uint64), ("candidates", C.c_uint64),
                 ("nnz_upper", C.c_uint64), ("energy", C.c_double), ("dav_iters", C.c_int),
                 ("dav_converged", C.c_int), ("ms_select", C.c_double), ("ms_build", C.c_double),
-                ("ms_davidson", C.c_double)]
+                ("ms_davidson", C.c_double), ("storage", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

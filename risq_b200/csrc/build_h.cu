@@ -285,8 +285,19 @@ constexpr int LOOKUP_MIN_GROUP = 256;
 // Kinds of structural hits, evaluated in batches.
 enum HitKind : int { K_SING_B = 0, K_SING_A = 1, K_DOUB_B = 2, K_DOUB_A = 3, K_OPP = 4 };
 
+// Vectors of the matrix-free sigma (MODE 5), internal order.
+struct SigmaIO {
+    const double* __restrict__ x;
+    double* __restrict__ y;
+    const double* __restrict__ diag;
+};
+
 // MODE 0: count structural candidates per row.  MODE 1/2/3: evaluate and store
 // FP64 / FP32 / FP32 + FP32 remainder.  MODE 4: evaluate, store the columns only.
+// MODE 5: matrix-free sigma, y_p = H_pp x_p + sum_q H_pq x_q over the row's
+// connections found and evaluated here (full rows, nothing stored); each lane sums its
+// hits in queue order and the warp adds the lanes in a fixed order, so a row's sum
+// does not depend on the schedule.
 //
 // One warp per row.  The scans visit candidates 32 at a time; only a minority are
 // connected, so evaluating Slater-Condon in place would run with a few lanes
@@ -301,7 +312,7 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
                                                     int32_t* __restrict__ row_len, int32_t* __restrict__ cols,
                                                     double* __restrict__ v64, float* __restrict__ v32,
                                                     float* __restrict__ vlo, int64_t row_lo, int64_t row_hi,
-                                                    int64_t base_off) {
+                                                    int64_t base_off, SigmaIO io) {
     constexpr int WARPS = 256 / 32;
     constexpr int QCAP = 64;  // < 32 pending + 32 new
     __shared__ int s_q[WARPS][2][QCAP];
@@ -320,8 +331,9 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
         if (p >= row_hi) break;
         const Bits<W> a = v.up_at(p), b = v.dn_at(p);
         const bool p_new = v.nsh == 0 || v.orig[p] >= v.nsh;
-        int64_t base = MODE ? row_start[p] - base_off : 0;
+        int64_t base = (MODE >= 1 && MODE <= 4) ? row_start[p] - base_off : 0;
         int count = 0;
+        double acc = 0.0;  // MODE 5
         int ns = 0, nd = 0;  // queue fill, warp-uniform
 
         auto store = [&](int64_t pos, int q, double val) {
@@ -349,9 +361,13 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
                 else if (kind == K_DOUB_A) { val = sc_double_same<W>(I, a, aq); ok = val != 0.0; }
                 else { val = sc_double_opp<W>(I, a, b, aq, bq); ok = val != 0.0; }
             }
-            const unsigned m = __ballot_sync(FULL, ok);
-            if (ok) store(base + count + __popc(m & lt), q, val);
-            count += __popc(m);
+            if constexpr (MODE == 5) {
+                if (ok) acc += val * __ldg(io.x + q);
+            } else {
+                const unsigned m = __ballot_sync(FULL, ok);
+                if (ok) store(base + count + __popc(m & lt), q, val);
+                count += __popc(m);
+            }
             const int rem = nq - take;
             int tq = 0;
             unsigned char tk = 0;
@@ -379,7 +395,7 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
         };
 
         // (0) elements kept from the previous build (pairs of old determinants)
-        if (!p_new && v.prev_inv_of_caller) {
+        if (MODE != 5 && !p_new && v.prev_inv_of_caller) {
             int op = v.prev_inv_of_caller[v.orig[p]];
             int64_t ps = v.prev_row_start[op];
             int pl = v.prev_row_len[op];
@@ -527,7 +543,11 @@ __global__ void __launch_bounds__(256) k_build_rows(SetView<W> v, Ints I, double
             if (ns > 0) flush(qs, ks, ns, ns);
             if (nd > 0) flush(qd, kd, nd, nd);
         }
-        if (lane == 0) {
+        if constexpr (MODE == 5) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(FULL, acc, o);
+            if (lane == 0) io.y[p] = io.diag[p] * io.x[p] + acc;
+        } else if (lane == 0) {
             // row capacities are rounded up to 4 elements so that every row starts on a
             // 16-byte (columns) / 32-byte (FP64 values) boundary for vector loads
             if (MODE == 0) cnt[p] = (count + 3) & ~3;
@@ -830,19 +850,19 @@ int launch_fill(risqgpu* h, const SetView<W>& v, const Ints& I, double thr, int 
     if (precision == RISQGPU_FP64)
         k_build_rows<W, 1><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start,
                                                               h->d_row_len, cols, v64, nullptr, nullptr, row_lo,
-                                                              row_hi, base);
+                                                              row_hi, base, SigmaIO{});
     else if (precision == RISQGPU_FP32)
         k_build_rows<W, 2><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start,
                                                               h->d_row_len, cols, nullptr, v32, nullptr, row_lo,
-                                                              row_hi, base);
+                                                              row_hi, base, SigmaIO{});
     else if (precision == RISQGPU_MIXED)
         k_build_rows<W, 3><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start,
                                                               h->d_row_len, cols, nullptr, v32, vlo, row_lo, row_hi,
-                                                              base);
+                                                              base, SigmaIO{});
     else
         k_build_rows<W, 4><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, nullptr, h->d_row_start,
                                                               h->d_row_len, cols, nullptr, nullptr, nullptr, row_lo,
-                                                              row_hi, base);
+                                                              row_hi, base, SigmaIO{});
     return check_launch(h, "fill rows");
 }
 
@@ -1067,7 +1087,7 @@ int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats*
     RQ_CUDA(h, cudaMemsetAsync(counter, 0, sizeof(int), h->stream));
     RQ_CUDA(h, cudaEventRecord(ev[0], h->stream));
     k_build_rows<W, 0><<<blocks, threads, 0, h->stream>>>(v, I, thr, upper, counter, cnt, nullptr, nullptr, nullptr,
-                                                          nullptr, nullptr, nullptr, 0, n, 0);
+                                                          nullptr, nullptr, nullptr, 0, n, 0, SigmaIO{});
     RQ_CUDA(h, cudaEventRecord(ev[1], h->stream));
     RQ_TRY(check_launch(h, "count rows"));
     {
@@ -1119,9 +1139,39 @@ int build_rows(risqgpu* h, int precision, int upper, double thr, risqgpu_hstats*
     return finish_build(h, precision, upper, cap, t0, t1, t2, ev, st);
 }
 
+// Matrix-free FP64 sigma: the build's connection search and Slater-Condon evaluation
+// run inside sigma, one warp per row over both triangles, so nothing but the
+// determinant tables is held (the replacement for stored columns when even those do
+// not fit).  The elements are those a full FP64 build with the same builder rule
+// stores, bit for bit.
+template <int W>
+int sigma_mf(risqgpu* h, const double* x, double* y) {
+    SetView<W> v = make_view<W>(h, false, nullptr);
+    v.nsh = 0;  // every pair, old and new determinants alike
+    Ints I{h->d_h1, h->d_h2, h->nuc};
+    static int cached_dev[2] = {-1, -1}, cached_blocks[2] = {0, 0};
+    if (cached_dev[W - 1] != h->device) {
+        int occ = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_build_rows<W, 5>, 256, 0);
+        cached_blocks[W - 1] = num_sms(h) * std::max(occ, 1);
+        cached_dev[W - 1] = h->device;
+    }
+    RQ_CUDA(h, cudaMemsetAsync(h->d_mf_counter, 0, sizeof(int), h->stream));
+    k_build_rows<W, 5><<<cached_blocks[W - 1], 256, 0, h->stream>>>(v, I, h->mf_thr, 0, h->d_mf_counter, nullptr,
+                                                                    nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                                    nullptr, 0, (int64_t)h->N, 0,
+                                                                    SigmaIO{x, y, h->d_diag});
+    return check_launch(h, "matrix-free sigma");
+}
+
 }  // namespace
 
+int sigma_matrix_free(risqgpu* h, const double* x, double* y) {
+    return h->W == 1 ? sigma_mf<1>(h, x, y) : sigma_mf<2>(h, x, y);
+}
+
 void free_csr(risqgpu* h) {
+    dfree(h->d_mf_counter);
     dfree(h->d_row_start); dfree(h->d_row_len); dfree(h->d_cols);
     dfree(h->d_val64); dfree(h->d_val32); dfree(h->d_val_lo);
     free_tiles(h);
@@ -1243,7 +1293,7 @@ int set_dets_impl(risqgpu* h, const uint64_t* dets, size_t n, size_t nsh, const 
 }
 
 int build_h_impl(risqgpu* h, int precision, int builder, risqgpu_hstats* st) {
-    if (precision < 0 || precision > 6) { h->err = "bad precision"; return RISQGPU_ERR_INVALID; }
+    if (precision < 0 || precision > RISQGPU_MATRIX_FREE) { h->err = "bad precision"; return RISQGPU_ERR_INVALID; }
     if (builder < 0 || builder > 2) { h->err = "bad builder"; return RISQGPU_ERR_INVALID; }
     if (h->N == 0) { h->err = "no determinants set"; return RISQGPU_ERR_INVALID; }
     if (h->nsh > 0 && (h->prev_precision != precision || precision >= RISQGPU_FP64_UPPER)) {
@@ -1254,6 +1304,25 @@ int build_h_impl(risqgpu* h, int precision, int builder, risqgpu_hstats* st) {
     double thr = fast ? 1e-12 : 0.0;
     auto t0 = std::chrono::steady_clock::now();
     free_csr(h);
+    if (precision == RISQGPU_MATRIX_FREE) {
+        // nothing to store: sigma finds and evaluates every row's elements itself
+        if (h->part_n > 1) {
+            h->err = "matrix-free storage has no row-block partition";
+            return RISQGPU_ERR_INVALID;
+        }
+        RQ_TRY(dalloc(h, h->d_mf_counter, 1));
+        h->precision = RISQGPU_MATRIX_FREE;
+        h->upper = false;
+        h->mf_thr = thr;
+        h->built = true;
+        h->nsh = 0;
+        if (st) {
+            std::memset(st, 0, sizeof(*st));
+            st->n_dets = h->N;
+            st->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        }
+        return RISQGPU_OK;
+    }
     // upper-triangle storage modes map onto the value types with the upper flag set
     int upper = precision >= RISQGPU_FP64_UPPER ? 1 : 0;
     int vprec = precision == RISQGPU_FP64_UPPER ? RISQGPU_FP64
@@ -1275,6 +1344,7 @@ int build_h_impl(risqgpu* h, int precision, int builder, risqgpu_hstats* st) {
 
 int export_upper_impl(risqgpu* h, int64_t* rowptr, int64_t* cols, double* vals, size_t cap, double* diag) {
     if (!h->built) { h->err = "no built matrix"; return RISQGPU_ERR_INVALID; }
+    if (h->precision == RISQGPU_MATRIX_FREE) { h->err = "a matrix-free build stores nothing to export"; return RISQGPU_ERR_INVALID; }
     const size_t n = h->N;
     if (cap < h->nnz_upper) { h->err = "export capacity too small"; return RISQGPU_ERR_CAPACITY; }
     std::vector<int64_t> rs(n + 1);
@@ -1428,7 +1498,10 @@ __global__ void k_rows_full(const int64_t* __restrict__ rows, int64_t k, const i
 int export_rows_impl(risqgpu* h, const int64_t* rows, size_t k, int64_t* out_r, int64_t* out_c, double* out_v,
                      size_t cap, size_t* count) {
     if (!h->built) { h->err = "no built matrix"; return RISQGPU_ERR_INVALID; }
-    if (h->precision == RISQGPU_COLS) { h->err = "row export needs stored values (not COLS)"; return RISQGPU_ERR_INVALID; }
+    if (h->precision == RISQGPU_COLS || h->precision == RISQGPU_MATRIX_FREE) {
+        h->err = "row export needs stored values (not COLS or MATRIX_FREE)";
+        return RISQGPU_ERR_INVALID;
+    }
     for (size_t i = 0; i < k; i++)
         if (rows[i] < 0 || (size_t)rows[i] >= h->N) { h->err = "row index out of range"; return RISQGPU_ERR_INVALID; }
     // rows must be distinct (each is exported once per stored element)

@@ -589,7 +589,8 @@ int davidson_impl(risqgpu* h, int nroots, const double* init, int ninit, double 
     }
     if (init && (ninit < 1 || ninit > space)) { h->err = "bad ninit"; return RISQGPU_ERR_INVALID; }
     if (init && nroots > 1 && ninit < nroots) { h->err = "ninit must be >= nroots for several roots"; return RISQGPU_ERR_INVALID; }
-    if (mode != RISQGPU_MODE_FP64 && (h->precision == RISQGPU_FP64 || h->precision == RISQGPU_COLS)) {
+    if (mode != RISQGPU_MODE_FP64 &&
+        (h->precision == RISQGPU_FP64 || h->precision == RISQGPU_COLS || h->precision == RISQGPU_MATRIX_FREE)) {
         h->err = "the FP32 sigma of MIXED / FP32 mode needs an FP32 or MIXED build";
         return RISQGPU_ERR_INVALID;
     }

@@ -277,11 +277,19 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
                 RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, 0, h->wf_diag.data()));
                 rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
             }
+            if (rc == RISQGPU_ERR_OOM && auto_prec && cur_prec == RISQGPU_COLS) {
+                // not even the columns fit: find and evaluate the elements inside sigma
+                if (verbose) std::fprintf(stderr, "[risqgpu] iter %d: columns do not fit, matrix-free from here\n", iter);
+                cur_prec = RISQGPU_MATRIX_FREE;
+                RQ_TRY(set_dets_impl(h, h->wf_dets.data(), N, 0, h->wf_diag.data()));
+                rc = build_h_impl(h, cur_prec, RISQGPU_BUILDER_AUTO, nullptr);
+            }
             if (rc != RISQGPU_OK) {
                 // the space outgrew every storage mode: log the selection that got that far
                 rec.n_dets = N;
                 rec.energy = NAN;
                 rec.dav_converged = -1;
+                rec.storage = -1;
                 h->var_log.push_back(rec);
                 return rc;
             }
@@ -302,6 +310,7 @@ int variational_impl(risqgpu* h, int nup, int ndn, int ncore, double eps_var, in
         }  // on non-convergence energy and coefficients stay (src/var/davidson.rs:109-111)
         auto t3 = clk::now();
         rec.n_dets = N;
+        rec.storage = cur_prec;
         rec.nnz_upper = h->nnz_upper;
         rec.energy = h->wf_energy;
         rec.dav_iters = ds.iters;

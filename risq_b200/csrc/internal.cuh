@@ -93,7 +93,7 @@ struct risqgpu {
     int ht_bits = 0;
 
     // sparse H: both triangles, rows in internal order, diagonal separate
-    int precision = -1;   // value storage: FP64, FP32, MIXED or COLS
+    int precision = -1;   // value storage: FP64, FP32, MIXED, COLS or MATRIX_FREE
     bool upper = false;   // only pairs with q > p (internal order) are stored
     bool built = false;
     int64_t* d_row_start = nullptr;  // N + 1 (segment starts; capacity per row)
@@ -105,6 +105,9 @@ struct risqgpu {
     size_t cap = 0;             // allocated element slots
     uint64_t nnz_full = 0;
     uint64_t nnz_upper = 0;
+    // matrix-free storage: the sigma's row counter and the builder's singles threshold
+    int* d_mf_counter = nullptr;
+    double mf_thr = 0.0;
 
     // Tiled upper-triangle storage (upper builds).  Rows are cut into panels of
     // 2^tile_rb consecutive rows and columns into windows of 2^tile_cb.  Each panel
@@ -118,7 +121,13 @@ struct risqgpu {
     int64_t n_tiles = 0;
     uint64_t n_dense_el = 0;          // stored pairs in dense tiles
     int64_t* d_panel_tile = nullptr;  // n_panels + 1: first tile of each panel
+    // sigma work units: runs of one panel's tiles of about equal pair counts, largest
+    // first; 3 int64 each: first tile, end tile, panel * 2 + (1 if the unit also takes
+    // the panel's leftover pairs)
+    int64_t n_units = 0;
+    int64_t* d_units = nullptr;
     int32_t* d_tile_win = nullptr;    // window of each tile
+    float* d_tile_bound = nullptr;    // FP32 values: largest row or column sum of |H| in each tile
     int32_t* d_tile_len = nullptr;    // elements of each tile
     int64_t* d_tile_off = nullptr;    // first element of each tile
     int64_t* d_left_off = nullptr;    // N: first leftover element of each row
@@ -277,6 +286,8 @@ int permute_out(risqgpu* h, const double* yi, double* y);
 // tiled upper-triangle storage (tiles.cu)
 int tile_shape(int64_t N, int& rb, int& cb);
 int sigma_tiles(risqgpu* h, const void* x, void* y, int kind);
+// FP64 sigma of a matrix-free build (build_h.cu), internal order
+int sigma_matrix_free(risqgpu* h, const double* x, double* y);
 // Sum `count` int64 values in place across the partition's ranks (the caller's all-reduce,
 // on the handle's stream).
 int part_allreduce(risqgpu* h, void* buf_dev, size_t count);
@@ -296,11 +307,13 @@ struct TileBuilder {
     size_t tile_cap = 0;
     int64_t el_cap = 0;
     int64_t el_next = 0, tile_next = 0;
+    std::vector<int64_t> panel_el;  // host: first element of each panel, and the end
     int begin(risqgpu* h, int64_t n_panels, int64_t element_capacity);
     template <typename VIN>
     int chunk(int64_t p_lo, int64_t p_hi, const int64_t* row_start, int64_t base, const int32_t* row_len,
               const int32_t* cols, const VIN* vin, const float* vlo_in, VIN* vout, float* vlo_out);
     int finish();
+    int make_units();
     ~TileBuilder();
 };
 

@@ -210,6 +210,13 @@ int sigma_device(risqgpu* h, const void* x, void* y, int kind) {
     const int64_t n = (int64_t)h->N;
     const int grid = spmv_grid(h);
     if (h->upper) return sigma_tiles(h, x, y, kind);
+    if (h->precision == RISQGPU_MATRIX_FREE) {
+        if (kind != 0) {
+            h->err = "a matrix-free build has only the FP64 sigma";
+            return RISQGPU_ERR_INVALID;
+        }
+        return sigma_matrix_free(h, (const double*)x, (double*)y);
+    }
     if (kind == 0) {
         const double* xd = (const double*)x;
         double* yd = (double*)y;
@@ -267,7 +274,10 @@ int sigma_host(risqgpu* h, const double* x, double* y, int nvec) {
 
 int self_energy_impl(risqgpu* h, double energy, double gmin, double* out) {
     if (!h->built) { h->err = "self energy before build"; return RISQGPU_ERR_INVALID; }
-    if (h->precision == RISQGPU_COLS) { h->err = "self energy needs stored values (not COLS)"; return RISQGPU_ERR_INVALID; }
+    if (h->precision == RISQGPU_COLS || h->precision == RISQGPU_MATRIX_FREE) {
+        h->err = "self energy needs stored values (not COLS or MATRIX_FREE)";
+        return RISQGPU_ERR_INVALID;
+    }
     if (!(gmin > 0.0)) { h->err = "gmin must be positive"; return RISQGPU_ERR_INVALID; }
     const int64_t n = (int64_t)h->N;
     double *si = nullptr, *sc = nullptr;

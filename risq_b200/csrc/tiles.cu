@@ -339,6 +339,51 @@ struct AccFloat {
     __device__ __forceinline__ static void add(T* a, T v) { atomicAdd(a, v); }
 };
 
+// Four FP32 sums added to four consecutive global floats (16-byte aligned) by one
+// vector reduction.
+__device__ __forceinline__ void red_add_v4(float* a, const float4 v) {
+    asm volatile("red.relaxed.gpu.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(a), "f"(v.x), "f"(v.y),
+                 "f"(v.z), "f"(v.w)
+                 : "memory");
+}
+
+// Adds the window sums src[0, n) (shared) to dst[0, n) (global), zeros skipped.  FP32
+// sums into a 16-byte aligned destination go four at a time through vector reductions,
+// a quarter of the L2 atomic operations.
+template <typename A>
+__device__ __forceinline__ void flush_window(typename A::T* __restrict__ dst, const typename A::T* __restrict__ src,
+                                             int n) {
+    using T = typename A::T;
+    int i0 = 0;
+    if constexpr (std::is_same<T, float>::value) {
+        if ((reinterpret_cast<uintptr_t>(dst) & 15u) == 0) {
+            const int n4 = n >> 2;
+            for (int i = threadIdx.x; i < n4; i += TT) {
+                const float4 a = reinterpret_cast<const float4*>(src)[i];
+                if (a.x != 0.f || a.y != 0.f || a.z != 0.f || a.w != 0.f) red_add_v4(dst + 4 * i, a);
+            }
+            i0 = 4 * n4;
+        }
+    }
+    for (int i = i0 + threadIdx.x; i < n; i += TT) {
+        const T a = src[i];
+        if (a != 0) A::add(dst + i, a);
+    }
+}
+
+// Stages x[0, n) into shared memory (16-byte vector loads when x is aligned).
+template <typename X>
+__device__ __forceinline__ void stage_window(X* __restrict__ dst, const X* __restrict__ x, int n) {
+    constexpr int PER = 16 / sizeof(X);
+    int i0 = 0;
+    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) {
+        const int nv = n / PER;
+        for (int i = threadIdx.x; i < nv; i += TT) reinterpret_cast<uint4*>(dst)[i] = __ldg(reinterpret_cast<const uint4*>(x) + i);
+        i0 = nv * PER;
+    }
+    for (int i = i0 + threadIdx.x; i < n; i += TT) dst[i] = x[i];
+}
+
 // Four consecutive stored values (16-byte aligned element index e) as the vector type.
 template <typename V, typename X, bool VLO>
 __device__ __forceinline__ void load4(const V* __restrict__ vals, const float* __restrict__ vlo, int64_t e,
@@ -361,7 +406,7 @@ __device__ __forceinline__ void load4(const V* __restrict__ vals, const float* _
 // A: accumulation policy.
 template <typename V, typename X, bool VLO, typename A>
 __global__ void __launch_bounds__(TT) k_sigma_tiles(
-    int64_t N, int64_t p_lo, int64_t p_hi, int rb, int cb, const int64_t* __restrict__ panel_tile,
+    int64_t N, int64_t n_units, const int64_t* __restrict__ units, int rb, int cb,
     const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
     const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len, const uint32_t* __restrict__ el_idx,
     const V* __restrict__ vals, const float* __restrict__ vlo, const X* __restrict__ x,
@@ -373,34 +418,31 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
     T* yJ = yP + R;
     X* xP = reinterpret_cast<X*>(yJ + C);
     X* xJ = xP + R;
-    __shared__ long long s_panel;
+    __shared__ long long s_unit;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t cmask = (uint32_t)C - 1u;
     const A ac(scalars);
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
     for (;;) {
-        if (threadIdx.x == 0) s_panel = p_lo + (long long)atomicAdd(counter, 1ull);
+        if (threadIdx.x == 0) s_unit = (long long)atomicAdd(counter, 1ull);
         __syncthreads();
-        const int64_t P = s_panel;
-        if (P >= p_hi) break;
+        const int64_t u = s_unit;
+        if (u >= n_units) break;
+        const int64_t tb = units[3 * u], te = units[3 * u + 1], pl = units[3 * u + 2];
+        const int64_t P = pl >> 1;
+        const bool with_left = (pl & 1) != 0;
         const int64_t r0 = P << rb;
         const int nr = (int)min((int64_t)R, N - r0);
-        for (int i = threadIdx.x; i < nr; i += TT) {
-            xP[i] = x[r0 + i];
-            yP[i] = 0;
-        }
+        stage_window<X>(xP, x + r0, nr);
+        for (int i = threadIdx.x; i < nr; i += TT) yP[i] = 0;
         __syncthreads();
-        const int64_t tb = panel_tile[P], te = panel_tile[P + 1];
         for (int64_t t = tb; t < te; t++) {
             const int64_t c0 = (int64_t)tile_win[t] << cb;
             const int w = (int)min((int64_t)C, N - c0);
             const int64_t e0 = tile_off[t];
             const int len = tile_len[t];
-#pragma unroll 4
-            for (int i = threadIdx.x; i < w; i += TT) {
-                xJ[i] = x[c0 + i];
-                yJ[i] = 0;
-            }
+            stage_window<X>(xJ, x + c0, w);
+            for (int i = threadIdx.x; i < w; i += TT) yJ[i] = 0;
             __syncthreads();
             // the unaligned head and tail one pair per thread, the 16-byte aligned body in
             // blocks of four consecutive pairs per thread (vector loads, coalesced across the
@@ -456,14 +498,11 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
                 if (two) sum_block(u2, v2);
             }
             __syncthreads();
-            for (int i = threadIdx.x; i < w; i += TT) {
-                const T a = yJ[i];
-                if (a != 0) A::add(acc + c0 + i, a);
-            }
+            flush_window<A>(acc + c0, yJ, w);
             __syncthreads();
         }
         // leftover pairs: one warp per row, private row sum, column sums by global atomics
-        for (int i = warp; i < nr; i += TT / 32) {
+        for (int i = warp; with_left && i < nr; i += TT / 32) {
             const int64_t s = left_off[r0 + i];
             const int len = left_len[r0 + i];
             const X xr = xP[i];
@@ -499,9 +538,200 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
             if (lane == 0 && len > 0) A::add(yP + i, ac.conv(rs));
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < nr; i += TT) {
-            const T a = yP[i];
-            if (a != 0) A::add(acc + r0 + i, a);
+        flush_window<A>(acc + r0, yP, nr);
+        __syncthreads();
+    }
+}
+
+// FP32 sigma with 32-bit integer shared windows.  Shared-memory integer atomics are
+// single instructions, where FP32 shared atomics are compare-and-swap loops, so each
+// tile's row and column window sums are formed in fixed point: every product is
+// rounded to a multiple of 2^-s_t, s_t chosen from the tile's bound (the largest sum
+// of |H| over one row or one column of the tile, times max |x|) so that no window sum
+// exceeds 2^30.  Each product then carries an error of at most 2^-31 of the tile's
+// largest window sum, below FP32 rounding of that sum.  Window sums go to FP32: the
+// row sums into the unit's FP32 row window, the column sums by vector reductions into
+// the global FP32 accumulator.  Leftover pairs as in k_sigma_tiles.
+__global__ void __launch_bounds__(TT) k_sigma_tiles_i32(
+    int64_t N, int64_t n_units, const int64_t* __restrict__ units, int rb, int cb,
+    const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
+    const float* __restrict__ tile_bound, const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len,
+    const uint32_t* __restrict__ el_idx, const float* __restrict__ vals, const float* __restrict__ x,
+    float* __restrict__ acc, double* __restrict__ scalars) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int R = 1 << rb, C = 1 << cb;
+    float* xP = reinterpret_cast<float*>(sm);
+    float* yP = xP + R;
+    int* yPt = reinterpret_cast<int*>(yP + R);
+    float* xJ = reinterpret_cast<float*>(yPt + R);
+    int* yJ = reinterpret_cast<int*>(xJ + C);
+    __shared__ long long s_unit;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t cmask = (uint32_t)C - 1u;
+    const float xmax = (float)__longlong_as_double(*reinterpret_cast<const long long*>(scalars));
+    unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
+    for (;;) {
+        if (threadIdx.x == 0) s_unit = (long long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const int64_t u = s_unit;
+        if (u >= n_units) break;
+        const int64_t tb = units[3 * u], te = units[3 * u + 1], pl = units[3 * u + 2];
+        const int64_t P = pl >> 1;
+        const bool with_left = (pl & 1) != 0;
+        const int64_t r0 = P << rb;
+        const int nr = (int)min((int64_t)R, N - r0);
+        stage_window<float>(xP, x + r0, nr);
+        for (int i = threadIdx.x; i < R; i += TT) {
+            yP[i] = 0.f;
+            yPt[i] = 0;
+        }
+        __syncthreads();
+        for (int64_t t = tb; t < te; t++) {
+            const int64_t c0 = (int64_t)tile_win[t] << cb;
+            const int w = (int)min((int64_t)C, N - c0);
+            const int64_t e0 = tile_off[t];
+            const int len = tile_len[t];
+            // fixed-point scale of this tile: window sums stay below 2^30
+            const float bt = tile_bound[t] * xmax;
+            int sh = 0;
+            if (bt > 0.f && isfinite(bt)) sh = 29 - ilogbf(bt);
+            sh = max(-100, min(100, sh));
+            const float sc = ldexpf(1.f, sh), inv = ldexpf(1.f, -sh);
+            stage_window<float>(xJ, x + c0, w);
+            for (int i = threadIdx.x; i < w; i += TT) yJ[i] = 0;
+            __syncthreads();
+            const int head = (int)min((int64_t)len, (4 - (e0 & 3)) & 3);
+            const int64_t eb = e0 + head;
+            const int nblk = (len - head) >> 2;
+            const int rest = len - head - 4 * nblk;
+            if ((int)threadIdx.x < head + rest) {
+                const int64_t e = (int)threadIdx.x < head ? e0 + threadIdx.x : eb + 4 * nblk + (threadIdx.x - head);
+                const uint32_t uu = __ldcs(el_idx + e);
+                const float v = __ldcs(vals + e) * sc;
+                const uint32_t lr = uu >> cb, lc = uu & cmask;
+                if (lr < (uint32_t)nr && lc < (uint32_t)w) {  // never false for a valid layout
+                    atomicAdd(yPt + lr, __float2int_rn(v * xJ[lc]));
+                    atomicAdd(yJ + lc, __float2int_rn(v * xP[lr]));
+                }
+            }
+            auto sum_block = [&](const uint4 u4, const float4 v4) {
+                const uint32_t uq[4] = {u4.x, u4.y, u4.z, u4.w};
+                const float vq[4] = {v4.x * sc, v4.y * sc, v4.z * sc, v4.w * sc};
+                uint32_t rcur = uq[0] >> cb;
+                int racc = 0;
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const uint32_t lr = uq[j] >> cb, lc = uq[j] & cmask;
+                    if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;  // never taken for a valid layout
+                    const int tr = __float2int_rn(vq[j] * xJ[lc]);
+                    atomicAdd(yJ + lc, __float2int_rn(vq[j] * xP[lr]));
+                    if (lr != rcur) {
+                        if (racc != 0 && rcur < (uint32_t)nr) atomicAdd(yPt + rcur, racc);
+                        rcur = lr;
+                        racc = 0;
+                    }
+                    racc += tr;
+                }
+                if (racc != 0 && rcur < (uint32_t)nr) atomicAdd(yPt + rcur, racc);
+            };
+            for (int bk = threadIdx.x; bk < nblk; bk += 2 * TT) {
+                const bool two = bk + TT < nblk;
+                const int64_t e1 = eb + 4 * (int64_t)bk, e2 = e1 + 4 * (int64_t)TT;
+                const uint4 u1 = __ldcs(reinterpret_cast<const uint4*>(el_idx + e1));
+                const float4 v1 = __ldcs(reinterpret_cast<const float4*>(vals + e1));
+                uint4 u2 = make_uint4(0, 0, 0, 0);
+                float4 v2 = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (two) {
+                    u2 = __ldcs(reinterpret_cast<const uint4*>(el_idx + e2));
+                    v2 = __ldcs(reinterpret_cast<const float4*>(vals + e2));
+                }
+                sum_block(u1, v1);
+                if (two) sum_block(u2, v2);
+            }
+            __syncthreads();
+            // column sums to the global accumulator, row sums into the unit's FP32 window
+            if ((reinterpret_cast<uintptr_t>(acc + c0) & 15u) == 0) {
+                for (int i = threadIdx.x; i < (w >> 2); i += TT) {
+                    const int4 a = reinterpret_cast<const int4*>(yJ)[i];
+                    if (a.x | a.y | a.z | a.w)
+                        red_add_v4(acc + c0 + 4 * i, make_float4((float)a.x * inv, (float)a.y * inv,
+                                                                 (float)a.z * inv, (float)a.w * inv));
+                }
+                for (int i = 4 * (w >> 2) + threadIdx.x; i < w; i += TT)
+                    if (yJ[i] != 0) atomicAdd(acc + c0 + i, (float)yJ[i] * inv);
+            } else {
+                for (int i = threadIdx.x; i < w; i += TT)
+                    if (yJ[i] != 0) atomicAdd(acc + c0 + i, (float)yJ[i] * inv);
+            }
+            for (int i = threadIdx.x; i < nr; i += TT) {
+                const int a = yPt[i];
+                if (a != 0) {
+                    yP[i] += (float)a * inv;  // row i belongs to this thread alone here
+                    yPt[i] = 0;
+                }
+            }
+            __syncthreads();
+        }
+        // leftover pairs: one warp per row, private row sum, column sums by global atomics
+        for (int i = warp; with_left && i < nr; i += TT / 32) {
+            const int64_t s = left_off[r0 + i];
+            const int len = left_len[r0 + i];
+            const float xr = xP[i];
+            float rs = 0.f;
+            for (int k = lane; k < len; k += 32) {
+                const uint32_t q = __ldcs(el_idx + s + k);
+                const float v = __ldcs(vals + s + k);
+                if (q >= (uint64_t)N) continue;  // never taken for a valid layout
+                rs += v * __ldg(x + q);
+                atomicAdd(acc + q, v * xr);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(FULL, rs, o);
+            if (lane == 0) yP[i] += rs;  // one warp per row
+        }
+        __syncthreads();
+        flush_window<AccFloat<float>>(acc + r0, yP, nr);
+        __syncthreads();
+    }
+}
+
+// Per tile: the largest sum of |value| over one of its rows or columns (FP32 values),
+// the bound that k_sigma_tiles_i32 scales its fixed point by.
+__global__ void __launch_bounds__(TT) k_tile_bounds(int64_t n_tiles, int rb, int cb,
+                                                   const int32_t* __restrict__ tile_len,
+                                                   const int64_t* __restrict__ tile_off,
+                                                   const uint32_t* __restrict__ el_idx,
+                                                   const float* __restrict__ vals, float* __restrict__ bound) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int R = 1 << rb, C = 1 << cb;
+    float* rs = reinterpret_cast<float*>(sm);
+    float* cs = rs + R;
+    __shared__ float s_max[TT / 32];
+    const uint32_t cmask = (uint32_t)C - 1u;
+    for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        for (int i = threadIdx.x; i < R + C; i += TT) rs[i] = 0.f;
+        __syncthreads();
+        const int64_t e0 = tile_off[t];
+        const int len = tile_len[t];
+        for (int k = threadIdx.x; k < len; k += TT) {
+            const uint32_t u = el_idx[e0 + k];
+            const float a = fabsf(vals[e0 + k]);
+            const uint32_t lr = u >> cb, lc = u & cmask;
+            if (lr < (uint32_t)R) atomicAdd(rs + lr, a);
+            atomicAdd(cs + lc, a);
+        }
+        __syncthreads();
+        float m = 0.f;
+        for (int i = threadIdx.x; i < R + C; i += TT) m = fmaxf(m, rs[i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(FULL, m, o));
+        if ((threadIdx.x & 31) == 0) s_max[threadIdx.x >> 5] = m;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float b = 0.f;
+            for (int k = 0; k < TT / 32; k++) b = fmaxf(b, s_max[k]);
+            // FP32 sums of |value| round down by at most a few ulps of the bound
+            bound[t] = b * (1.f + 0x1p-16f);
         }
         __syncthreads();
     }
@@ -635,17 +865,17 @@ int launch_tiles_acc(risqgpu* h, const X* x, X* y, const V* vals, const float* v
     }
     int occ = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem_k);
-    const int64_t own = h->part_p_hi - h->part_p_lo;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(own, (int64_t)num_sms(h) * std::max(occ, 1)));
+    const int grid =
+        (int)std::max<int64_t>(1, std::min<int64_t>(h->n_units, (int64_t)num_sms(h) * std::max(occ, 1)));
     T* acc = reinterpret_cast<T*>(h->d_acc);  // N entries of at most 8 bytes
     RQ_CUDA(h, cudaMemsetAsync(h->d_acc, 0, sizeof(long long) * N, h->stream));
     RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double), h->stream));
     k_absmax<X><<<grid_n(h, N), 256, 0, h->stream>>>(x, N, reinterpret_cast<unsigned long long*>(h->d_sig_scalars));
     k_fixed_scale<<<1, 1, 0, h->stream>>>(h->d_sig_scalars, h->h_row_abs_max,
                                          std::is_same<X, float>::value ? 100 : 1000, top);
-    kern<<<grid, TT, smem_k, h->stream>>>(N, h->part_p_lo, h->part_p_hi, h->tile_rb, h->tile_cb, h->d_panel_tile,
-                                       h->d_tile_win, h->d_tile_len, h->d_tile_off, h->d_left_off, h->d_left_len,
-                                       h->d_el_idx, vals, vlo, x, acc, h->d_sig_scalars);
+    kern<<<grid, TT, smem_k, h->stream>>>(N, h->n_units, h->d_units, h->tile_rb, h->tile_cb, h->d_tile_win,
+                                       h->d_tile_len, h->d_tile_off, h->d_left_off, h->d_left_len, h->d_el_idx, vals,
+                                       vlo, x, acc, h->d_sig_scalars);
     RQ_TRY(check_launch(h, "sigma (tiles)"));
     // with a row-block partition every rank summed its own panels: the exact integer
     // sums are added across the ranks
@@ -654,13 +884,47 @@ int launch_tiles_acc(risqgpu* h, const X* x, X* y, const V* vals, const float* v
     return check_launch(h, "sigma (tiles)");
 }
 
-// FP32 vectors sum in FP32 with native shared and global atomics (order-dependent
-// last bits, 30 % faster than fixed point at config 1) unless the handle asked for
-// reproducible sums or is partitioned (the ranks' sums must add exactly); FP64
-// vectors always sum in fixed point (no slower there).
+int launch_tiles_i32(risqgpu* h, const float* x, float* y) {
+    const int64_t N = (int64_t)h->N;
+    const int R = 1 << h->tile_rb, C = 1 << h->tile_cb;
+    const size_t smem = (size_t)(3 * R + 2 * C) * 4;
+    static int attr_set[64] = {0};
+    const int dev = h->device & 63;
+    if (attr_set[dev] < (int)smem) {
+        RQ_CUDA(h, cudaFuncSetAttribute(k_sigma_tiles_i32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set[dev] = (int)smem;
+    }
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sigma_tiles_i32, TT, smem);
+    const int grid =
+        (int)std::max<int64_t>(1, std::min<int64_t>(h->n_units, (int64_t)num_sms(h) * std::max(occ, 1)));
+    float* acc = reinterpret_cast<float*>(h->d_acc);
+    RQ_CUDA(h, cudaMemsetAsync(h->d_acc, 0, sizeof(long long) * N, h->stream));
+    RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double), h->stream));
+    k_absmax<float><<<grid_n(h, N), 256, 0, h->stream>>>(x, N, reinterpret_cast<unsigned long long*>(h->d_sig_scalars));
+    k_fixed_scale<<<1, 1, 0, h->stream>>>(h->d_sig_scalars, h->h_row_abs_max, 100, 61);
+    k_sigma_tiles_i32<<<grid, TT, smem, h->stream>>>(N, h->n_units, h->d_units, h->tile_rb, h->tile_cb, h->d_tile_win,
+                                                     h->d_tile_len, h->d_tile_off, h->d_tile_bound, h->d_left_off,
+                                                     h->d_left_len, h->d_el_idx, h->d_val32, x, acc,
+                                                     h->d_sig_scalars);
+    RQ_TRY(check_launch(h, "sigma (tiles, FP32)"));
+    k_fixed_finish<float, float><<<grid_n(h, N), 256, 0, h->stream>>>(N, h->d_diag, x, acc, h->d_sig_scalars, y);
+    return check_launch(h, "sigma (tiles, FP32)");
+}
+
+#ifndef RISQ_SIGMA32_I32
+#define RISQ_SIGMA32_I32 1
+#endif
+
+// FP32 vectors sum with 32-bit integer shared windows (k_sigma_tiles_i32) unless the
+// handle asked for reproducible sums or is partitioned (the ranks' sums must add
+// exactly): those, and FP64 vectors, sum in 64-bit fixed point.
 template <typename V, typename X, bool VLO>
 int launch_tiles(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo) {
     const bool flt = std::is_same<X, float>::value && !h->reproducible && h->part_n == 1;
+    if constexpr (std::is_same<X, float>::value) {
+        if (flt && RISQ_SIGMA32_I32 && h->d_tile_bound) return launch_tiles_i32(h, x, y);
+    }
     if (flt) return launch_tiles_acc<V, X, VLO, AccFloat<X>>(h, x, y, vals, vlo, 61);
     return launch_tiles_acc<V, X, VLO, AccExact<X>>(h, x, y, vals, vlo, 61);
 }
@@ -722,6 +986,7 @@ int TileBuilder::begin(risqgpu* h_, int64_t n_panels, int64_t element_capacity) 
     RQ_CUDA(h, cudaMemsetAsync(absmax, 0, sizeof(unsigned long long), h->stream));
     tile_cap = 0;
     el_next = tile_next = 0;
+    panel_el.assign((size_t)n_panels + 1, 0);
     return RISQGPU_OK;
 }
 
@@ -764,6 +1029,8 @@ int TileBuilder::chunk(int64_t p_lo, int64_t p_hi, const int64_t* row_start, int
     RQ_CUDA(h, cudaMemcpyAsync(last + 1, nel + np - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
     RQ_CUDA(h, cudaMemcpyAsync(last + 2, t_off + np - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
     RQ_CUDA(h, cudaMemcpyAsync(last + 3, nt64 + np - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, h->stream));
+    RQ_CUDA(h, cudaMemcpyAsync(panel_el.data() + p_lo, el_off, sizeof(int64_t) * np, cudaMemcpyDeviceToHost,
+                               h->stream));
     RQ_TRY(sync(h, "tile offsets"));
     const int64_t el_end = last[0] + last[1], t_end = last[2] + last[3];
     if (el_end > el_cap) {
@@ -820,11 +1087,74 @@ int TileBuilder::finish() {
         RQ_TRY(sync(h, "dense pairs"));
         h->n_dense_el = (uint64_t)v;
     }
+    RQ_TRY(make_units());
+    if (h->d_val32 && tile_next > 0) {
+        const int R = 1 << h->tile_rb, C = 1 << h->tile_cb;
+        const size_t smem = (size_t)(R + C) * sizeof(float);
+        RQ_TRY(dalloc(h, h->d_tile_bound, (size_t)tile_next));
+        RQ_CUDA(h, cudaFuncSetAttribute(k_tile_bounds, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const int grid = (int)std::min<int64_t>(tile_next, (int64_t)num_sms(h) * 8);
+        k_tile_bounds<<<grid, TT, smem, h->stream>>>(tile_next, h->tile_rb, h->tile_cb, h->d_tile_len, h->d_tile_off,
+                                                     h->d_el_idx, h->d_val32, h->d_tile_bound);
+        RQ_TRY(check_launch(h, "tile bounds"));
+    }
     RQ_TRY(dalloc(h, h->d_acc, (size_t)N));
     RQ_TRY(dalloc(h, h->d_sig_scalars, 4));
     dfree(row_abs);
     dfree(absmax);
     h->tiled = true;
+    return RISQGPU_OK;
+}
+
+// Sigma work units: each panel's tiles cut into runs of about `target` pairs (the
+// panel's leftover pairs go with its last run), largest first, so that the CTAs that
+// take units from a counter finish together even when a set has few, uneven panels.
+int TileBuilder::make_units() {
+    const int64_t p_lo = h->part_p_lo, p_hi = h->part_p_hi;
+    panel_el[(size_t)p_hi] = el_next;
+    std::vector<int64_t> pt((size_t)(p_hi - p_lo) + 1);
+    std::vector<int32_t> tl((size_t)tile_next);
+    RQ_CUDA(h, cudaMemcpyAsync(pt.data(), h->d_panel_tile + p_lo, sizeof(int64_t) * pt.size(), cudaMemcpyDeviceToHost,
+                               h->stream));
+    if (tile_next > 0)
+        RQ_CUDA(h, cudaMemcpyAsync(tl.data(), h->d_tile_len, sizeof(int32_t) * tl.size(), cudaMemcpyDeviceToHost,
+                                   h->stream));
+    RQ_TRY(sync(h, "sigma units"));
+    const int64_t total = el_next - panel_el[(size_t)p_lo];
+    const int64_t target = std::max<int64_t>(32768, total / ((int64_t)num_sms(h) * 16));
+    struct Unit { int64_t tb, te, pl, w; };
+    std::vector<Unit> us;
+    for (int64_t P = p_lo; P < p_hi; P++) {
+        const int64_t tb = pt[(size_t)(P - p_lo)], te = pt[(size_t)(P - p_lo) + 1];
+        const int64_t pairs = panel_el[(size_t)P + 1] - panel_el[(size_t)P];
+        if (pairs == 0) continue;
+        int64_t dense = 0;
+        for (int64_t t = tb; t < te; t++) dense += tl[(size_t)t];
+        int64_t start = tb, acc = 0;
+        for (int64_t t = tb; t < te; t++) {
+            acc += tl[(size_t)t];
+            if (acc >= target && t + 1 < te) {
+                us.push_back({start, t + 1, 2 * P, acc});
+                start = t + 1;
+                acc = 0;
+            }
+        }
+        us.push_back({start, te, 2 * P + 1, acc + (pairs - dense)});
+    }
+    std::stable_sort(us.begin(), us.end(), [](const Unit& a, const Unit& b) { return a.w > b.w; });
+    std::vector<int64_t> flat(3 * us.size());
+    for (size_t i = 0; i < us.size(); i++) {
+        flat[3 * i] = us[i].tb;
+        flat[3 * i + 1] = us[i].te;
+        flat[3 * i + 2] = us[i].pl;
+    }
+    h->n_units = (int64_t)us.size();
+    if (!us.empty()) {
+        RQ_TRY(dalloc(h, h->d_units, flat.size()));
+        RQ_CUDA(h, cudaMemcpyAsync(h->d_units, flat.data(), sizeof(int64_t) * flat.size(), cudaMemcpyHostToDevice,
+                                   h->stream));
+        RQ_TRY(sync(h, "sigma units"));
+    }
     return RISQGPU_OK;
 }
 
@@ -872,6 +1202,9 @@ int tiles_rows(risqgpu* h, const uint32_t* mark, int64_t* out_r, int64_t* out_c,
 
 void free_tiles(risqgpu* h) {
     dfree(h->d_panel_tile);
+    dfree(h->d_tile_bound);
+    dfree(h->d_units);
+    h->n_units = 0;
     dfree(h->d_tile_win);
     dfree(h->d_tile_len);
     dfree(h->d_tile_off);

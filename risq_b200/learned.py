@@ -22,6 +22,15 @@ forward / backward kernels (log-space squared error).
 Features (the inference kernel computes the same, mlp.cu): 2n occupations as +1/-1
 (alpha orbitals, then beta), (H_ii - E - mu_e) * s_e and
 (sum of occupied h_pp - mu_h) * s_h.
+
+Orbital-count-independent networks.  A network of the native layout is tied to one
+orbital count n.  The universal layout gives every spin NMAX = 32 slots, slot k
+holding the orbital with the k-th lowest h_pp (absent orbitals read 0), and replaces
+the sum of occupied h_pp by its mean over the electrons.  A universal network trained
+on systems of one or several orbital counts is turned, for a given system, into the
+exactly equivalent native network (`adapt`: W1's occupation columns gathered by
+orbital rank, the normalisation of the h_pp feature rescaled by the electron count),
+so the device kernels serve both.  Slots no training system had stay at weight 0.
 """
 from __future__ import annotations
 
@@ -35,6 +44,7 @@ from . import _capi as A
 from .fcidump import Integrals, dets_to_ints
 
 HIDDEN = 128
+NMAX = 32  # orbital slots per spin of the universal layout
 DATA_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 
 
@@ -80,9 +90,17 @@ class PrecondMLP:
         z = np.load(path)
         return cls(int(z["norb"]), int(z["hidden"]), z["params"].astype(np.float32), z["fnorm"].astype(np.float32))
 
+    @staticmethod
+    def pack(W1, b1, W2, b2, W3, b3):
+        return np.concatenate([np.ravel(W1), b1, np.ravel(W2), b2, W3, np.ravel(b3)]).astype(np.float32)
+
 
 def default_model_path(norb):
     return os.path.join(DATA_DIR, f"precond_mlp_n{norb}.npz")
+
+
+def universal_model_path():
+    return os.path.join(DATA_DIR, f"precond_mlp_u{NMAX}.npz")
 
 
 def load_default(norb):
@@ -123,6 +141,53 @@ def raw_features(dets, diag, energy, ints: Integrals):
     out[:, 2 * n] = (np.asarray(diag, dtype=np.float64) - energy).astype(np.float32)
     out[:, 2 * n + 1] = (up.astype(np.float32) @ hpp) + (dn.astype(np.float32) @ hpp)
     return out
+
+
+def orbital_ranks(ints: Integrals):
+    """rank[o]: position of orbital o in ascending h_pp order (ties by index)."""
+    hpp = np.array([ints.h(k, k) for k in range(ints.norb)], dtype=np.float64)
+    order = np.argsort(hpp, kind="stable")
+    rank = np.empty(ints.norb, dtype=np.int64)
+    rank[order] = np.arange(ints.norb)
+    return rank
+
+
+def n_electrons(dets):
+    d = np.asarray(dets[:1], dtype=np.uint64)
+    return int(sum(bin(int(w)).count("1") for w in d[0]))
+
+
+def universal_features(dets, diag, energy, ints: Integrals):
+    """(N, 2 NMAX + 2) float32 features of the universal layout before normalisation:
+    occupations by orbital rank, H_ii - E, mean occupied h_pp."""
+    n = ints.norb
+    if n > NMAX:
+        raise ValueError(f"the universal layout holds at most {NMAX} orbitals")
+    raw = raw_features(dets, diag, energy, ints)
+    rank = orbital_ranks(ints)
+    out = np.zeros((raw.shape[0], 2 * NMAX + 2), dtype=np.float32)
+    out[:, rank] = raw[:, :n]
+    out[:, NMAX + rank] = raw[:, n:2 * n]
+    out[:, 2 * NMAX] = raw[:, 2 * n]
+    out[:, 2 * NMAX + 1] = raw[:, 2 * n + 1] / n_electrons(dets)
+    return out
+
+
+def adapt(model: PrecondMLP, ints: Integrals, nel: int) -> PrecondMLP:
+    """The native network for a system of ints.norb orbitals and nel electrons that
+    computes exactly what the universal network computes on its universal features."""
+    if model.norb != NMAX:
+        raise ValueError("adapt takes a network of the universal layout")
+    n = ints.norb
+    rank = orbital_ranks(ints)
+    W1u, b1, W2, b2, W3, b3 = model.split()
+    W1 = np.zeros((model.hidden, 2 * n + 2), dtype=np.float32)
+    W1[:, :n] = W1u[:, rank]
+    W1[:, n:2 * n] = W1u[:, NMAX + rank]
+    W1[:, 2 * n:] = W1u[:, 2 * NMAX:]
+    fn = model.fnorm.astype(np.float64)
+    fnorm = np.array([fn[0], fn[1], fn[2] * nel, fn[3] / nel], dtype=np.float32)
+    return PrecondMLP(n, model.hidden, PrecondMLP.pack(W1, b1, W2, b2, W3, b3), fnorm)
 
 
 def normalise(feats, fnorm):
@@ -192,7 +257,8 @@ def target_factors(diag, S, energy):
     return np.where(gap > 0, np.clip(f, 0.25, 4.0), 1.0).astype(np.float32)
 
 
-def training_samples(gpu, dets, diag, ints, n_energies=12, per_energy=50000, rng=None, max_iter=2000):
+def training_samples(gpu, dets, diag, ints, n_energies=12, per_energy=50000, rng=None, max_iter=2000,
+                     universal=False):
     """(features, targets, weights) of one training system with a built FP64 matrix."""
     rng = rng or np.random.default_rng(0)
     lams = []
@@ -204,7 +270,7 @@ def training_samples(gpu, dets, diag, ints, n_energies=12, per_energy=50000, rng
     feats, targets = [], []
     for E in pick:
         idx = np.sort(rng.choice(N, size=min(per_energy, N), replace=False))
-        feats.append(raw_features(dets[idx], diag[idx], E, ints))
+        feats.append((universal_features if universal else raw_features)(dets[idx], diag[idx], E, ints))
         targets.append(f[idx])
     F = np.concatenate(feats)
     return F, np.concatenate(targets), np.ones(len(F), dtype=np.float32), dict(energy=lam_star, iters=iters)
@@ -238,9 +304,10 @@ def train(model: PrecondMLP, feats, target, weight, epochs=20, batch=4096, lr=1e
 
 
 def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, device=0, n_energies=12,
-                       per_energy=50000, log=print):
+                       per_energy=50000, log=print, universal=False):
     """systems: list of (ints, dets, diag).  Builds the samples (FP64 matrix and FP64
-    DPR Davidson per system), fits the feature normalisation and trains a fresh network."""
+    DPR Davidson per system), fits the feature normalisation and trains a fresh network
+    (universal: of the universal layout, norb ignored)."""
     from .gpu import GpuHam
     F, T, Wt = [], [], []
     rng = np.random.default_rng(seed)
@@ -249,7 +316,7 @@ def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, de
             g.set_dets(dets, 0, diag)
             g.build(A.FP64)
             f, t, w, info = training_samples(g, dets, diag, ints, n_energies=n_energies, per_energy=per_energy,
-                                             rng=rng)
+                                             rng=rng, universal=universal)
         F.append(f); T.append(t); Wt.append(w)
         log(f"# training system {k}: {len(dets)} dets, E = {info['energy']:.8f} after {info['iters']} DPR "
             f"iterations, {len(t)} samples, target factor median {np.median(t):.3f}")
@@ -257,7 +324,16 @@ def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, de
     n2 = raw.shape[1] - 2
     mu_e, sd_e = float(raw[:, n2].mean()), float(raw[:, n2].std() + 1e-6)
     mu_h, sd_h = float(raw[:, n2 + 1].mean()), float(raw[:, n2 + 1].std() + 1e-6)
-    model = PrecondMLP.init(norb, seed=seed, fnorm=[mu_e, 1.0 / sd_e, mu_h, 1.0 / sd_h])
+    model = PrecondMLP.init(NMAX if universal else norb, seed=seed, fnorm=[mu_e, 1.0 / sd_e, mu_h, 1.0 / sd_h])
+    if universal:
+        # slots that no training system fills keep weight 0, so that they add nothing
+        # for larger systems
+        W1, b1, W2, b2, W3, b3 = model.split()
+        nmax_seen = max(ints.norb for ints, _, _ in systems)
+        W1 = W1.copy()
+        W1[:, nmax_seen:NMAX] = 0.0
+        W1[:, NMAX + nmax_seen:2 * NMAX] = 0.0
+        model.params = PrecondMLP.pack(W1, b1, W2, b2, W3, b3)
     feats = normalise(raw, model.fnorm)
     hist = train(model, feats, np.concatenate(T), np.concatenate(Wt), epochs=epochs, batch=batch, lr=lr, seed=seed,
                  device=device)
@@ -265,5 +341,6 @@ def train_from_systems(systems, norb, epochs=30, batch=4096, lr=1e-3, seed=0, de
 
 
 __all__ = ["PrecondMLP", "install", "device_factors", "raw_features", "normalise", "dpr_trajectory",
+           "NMAX", "orbital_ranks", "universal_features", "adapt", "n_electrons",
            "self_energy", "target_factors", "training_samples", "grad", "train", "train_from_systems",
-           "load_default", "default_model_path", "dets_to_ints"]
+           "load_default", "default_model_path", "universal_model_path", "dets_to_ints"]

@@ -9,6 +9,12 @@ library's device variational stage, and per-determinant target factors from the
 second-order self-energy at the converged FP64 Davidson energy, with features taken
 at the Ritz values of the FP64 DPR trajectory (risq_b200.learned).  The network is then evaluated on seed 0
 (held out): Davidson iterations and time with and without it.
+
+--universal trains a network of the orbital-count-independent layout
+(risq_b200.learned.adapt), which can be evaluated on a system of another size:
+
+    python -m risq_b200.train_precond --universal --norb 20 --nel 8 --eps 1e-3 --seeds 1-8 \
+        --eval-norb 24 --eval-nel 10 --eval-eps 1e-3
 """
 from __future__ import annotations
 
@@ -41,6 +47,10 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--out", default=None)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--universal", action="store_true", help="orbital-count-independent layout")
+    ap.add_argument("--eval-norb", type=int, default=None)
+    ap.add_argument("--eval-nel", type=int, default=None)
+    ap.add_argument("--eval-eps", type=float, default=None)
     args = ap.parse_args()
     t0 = time.time()
     systems = []
@@ -52,17 +62,19 @@ def main():
         systems.append((ints, dets, diag))
     model, hist = learned.train_from_systems(systems, args.norb, epochs=args.epochs, lr=args.lr,
                                              n_energies=args.n_energies, per_energy=args.per_energy,
-                                             device=args.device)
+                                             device=args.device, universal=args.universal)
     print("# loss per epoch:", " ".join(f"{x:.4g}" for x in hist), flush=True)
-    out = args.out or learned.default_model_path(args.norb)
+    out = args.out or (learned.universal_model_path() if args.universal else learned.default_model_path(args.norb))
     model.save(out)
-    # held-out evaluation on seed 0
-    ints = synthetic_integrals(args.norb, 0)
+    # held-out evaluation on seed 0 (another orbital count for a universal network)
+    en, ee = args.eval_norb or args.norb, args.eval_nel or args.nel
+    eps = args.eval_eps or args.eps
+    ints = synthetic_integrals(en, 0)
     res = {}
     with GpuHam(ints, args.device) as g:
-        e, dets, c, diag, log = g.variational(args.nel, args.nel, args.eps, dav_max_iter=2000, precision=-1)
+        e, dets, c, diag, log = g.variational(ee, ee, eps, dav_max_iter=2000, precision=-1)
         g.set_dets(dets, 0, diag)
-        learned.install(g, model)
+        learned.install(g, learned.adapt(model, ints, 2 * ee) if args.universal else model)
         for prec, mode, pc, name in [(A.FP64, A.MODE_FP64, A.PRECOND_DPR, "fp64_dpr"),
                                      (A.FP64, A.MODE_FP64, A.PRECOND_LEARNED, "fp64_learned"),
                                      (A.MIXED, A.MODE_MIXED, A.PRECOND_DPR, "mixed_dpr"),
@@ -76,8 +88,8 @@ def main():
     e0 = res["fp64_dpr"]["energy"]
     for v in res.values():
         v["dE_uHa"] = abs(v["energy"] - e0) * 1e6
-    print(json.dumps({"held_out_seed": 0, "n_dets": int(len(dets)), "train_seconds": time.time() - t0,
-                      "results": res}))
+    print(json.dumps({"held_out_seed": 0, "eval": dict(norb=en, nel=ee, eps=eps), "universal": args.universal,
+                      "n_dets": int(len(dets)), "train_seconds": time.time() - t0, "results": res}))
 
 
 if __name__ == "__main__":

@@ -75,3 +75,30 @@ def test_target_factors():
     assert abs(f[3] - 4.0) < 1e-6           # denominator held at gap / 16 -> clip end
     assert f[4] == 4.0
     assert abs(f[5] - 2.0) < 1e-6
+
+
+def test_adapted_network_equals_universal_network():
+    """A universal-layout network (orbitals by h_pp rank, mean occupied h_pp) and its
+    adaptation to one system's native layout give the same factors."""
+    from risq_b200 import learned
+    rng = np.random.default_rng(3)
+    for norb, nel in [(12, 6), (24, 10)]:
+        ints = synthetic_integrals(norb, 4)
+        rows = []
+        for _ in range(300):
+            up = sum(1 << int(b) for b in rng.choice(norb, nel, replace=False))
+            dn = sum(1 << int(b) for b in rng.choice(norb, nel, replace=False))
+            rows.append((up, dn))
+        dets = dets_from_ints(rows)
+        diag = rng.uniform(-5.0, 5.0, len(dets))
+        u = PrecondMLP.init(learned.NMAX, seed=2, fnorm=[0.5, 0.7, -3.0, 0.4])
+        u.params = (u.params + 0.05 * rng.standard_normal(u.params.shape)).astype(np.float32)
+        a = learned.adapt(u, ints, 2 * nel)
+        assert a.n_in == 2 * norb + 2
+        Xu = normalise(learned.universal_features(dets, diag, -1.0, ints), u.fnorm)
+        Xa = normalise(raw_features(dets, diag, -1.0, ints), a.fnorm)
+        fu = mlp_ref.factors(u.params, Xu, u.n_in, u.hidden)
+        fa = mlp_ref.factors(a.params, Xa, a.n_in, a.hidden)
+        # the same sums up to FP32 order (an activation may round to the neighbouring BF16 value)
+        np.testing.assert_allclose(fa, fu, rtol=2e-3, atol=1e-6)
+        assert np.std(fu) > 1e-3

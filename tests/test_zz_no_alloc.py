@@ -24,7 +24,7 @@ def _noalloc(g, xd, yd):
     return lib.risqgpu_sigma_noalloc(g._h, ctypes.c_void_p(xd.data_ptr()), ctypes.c_void_p(yd.data_ptr()))
 
 
-@pytest.mark.parametrize("prec", [_capi.FP64, _capi.FP64_UPPER, _capi.MIXED_UPPER])
+@pytest.mark.parametrize("prec", [_capi.FP64, _capi.FP64_UPPER, _capi.MIXED_UPPER, _capi.MATRIX_FREE])
 def test_sigma_noalloc_matches_sigma_on_two_calls(prec):
     import torch
 
