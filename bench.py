@@ -75,6 +75,11 @@ CPU_SAMPLE_MAX = 150_000
 # memory of FP64 ones.
 THICK_SPACE = (32, 8)
 THICK_MIN_DETS = 1_000_000
+# From this size both paths store the upper triangle in tiles even where both
+# triangles would fit: the tiled sigma is the faster one there (n20 eps 1e-3, 551,147
+# dets: FP32 0.88 ms against 1.43 ms for both triangles; n24 HCI iteration 4,
+# 5,042,871 dets: FP64 27.4 ms against 38.2 ms) and holds half the bytes.
+UPPER_MIN_DETS = 500_000
 
 
 def product_space(n_dets, nroots=1):
@@ -363,7 +368,7 @@ def main():
         return a.elapsed_time(b), out
 
     if args.sigma_only:
-        prec = _capi.MIXED_UPPER if args.storage == "upper" or world > 1 else _capi.MIXED
+        prec = _capi.MIXED_UPPER if args.storage == "upper" or world > 1 or N >= UPPER_MIN_DETS else _capi.MIXED
         hs = g.build(prec)
         x32 = torch.randn(N, dtype=torch.float32, device="cuda")
         y32 = torch.empty_like(x32)
@@ -382,7 +387,8 @@ def main():
 
     # product path storage: FP32 + FP32 remainder rows when both triangles fit, else the
     # upper triangle (the reference's SparseMatUpperTri layout, regrouped into tiles)
-    upper_only = args.storage == "upper" or world > 1  # the partition splits upper-triangle storage
+    # the partition splits upper-triangle storage
+    upper_only = args.storage == "upper" or world > 1 or N >= UPPER_MIN_DETS
     precm = first_fitting([_capi.MIXED_UPPER] if upper_only else [_capi.MIXED, _capi.MIXED_UPPER])
 
     def solve(prec, mode, pc, space):
@@ -484,13 +490,14 @@ def main():
 
     # algorithmic bytes of one sigma: values + int32 column / element index of every stored
     # element, per row its start and length (12 B), x and the diagonal read once, y written
-    # once; tiled upper storage also reads 16 B per tile header; the recomputing kernel
-    # reads both strings of every determinant once (N * 16 B)
+    # once; tiled upper storage also reads 16 B per tile header (20 B for the FP32 sigma,
+    # which reads each tile's bound); the recomputing kernel reads both strings of every
+    # determinant once (N * 16 B)
     def sigma_bytes(prec, s_v, s_x, n_tiles):
         if prec in (_capi.FP64, _capi.MIXED, _capi.FP32):
             return nnz_f * (s_v + 4) + N * 12 + N * (2 * s_x + 8)
         if prec in (_capi.FP64_UPPER, _capi.MIXED_UPPER, _capi.FP32_UPPER):
-            return nnz_u * (s_v + 4) + N * 12 + N * (2 * s_x + 8) + 16 * n_tiles
+            return nnz_u * (s_v + 4) + N * 12 + N * (2 * s_x + 8) + (20 if s_x == 4 else 16) * n_tiles
         return nnz_f * 4 + N * 12 + N * (2 * s_x + 8) + N * 16
 
     b_sig = sigma_bytes(prec64, 8, 8, tiles64)
@@ -533,8 +540,9 @@ def main():
         sd, sg = dets[:n_s], diag[:n_s]
         g.set_partition(0, 1)  # the sample is solved by rank 0 alone
         g.set_dets(sd, 0, sg)
-        pm_s = _capi.MIXED if not upper_only else _capi.MIXED_UPPER
-        p64_s = _capi.FP64 if not upper_only else _capi.FP64_UPPER
+        up_s = args.storage == "upper" or n_s >= UPPER_MIN_DETS
+        pm_s = _capi.MIXED_UPPER if up_s else _capi.MIXED
+        p64_s = _capi.FP64_UPPER if up_s else _capi.FP64
         for _ in range(2):  # warm-up, then timed
             ms_sp, (_, r_sp) = timed(lambda: solve(pm_s, _capi.MODE_MIXED, precond, product_space(n_s)))
             ms_s64, (hs_s64, r_s64) = timed(lambda: solve(p64_s, _capi.MODE_FP64, _capi.PRECOND_DPR, (0, 0)))

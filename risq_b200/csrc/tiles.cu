@@ -13,15 +13,17 @@
 // two shared-memory updates and the global traffic per tile is one coalesced read
 // of x and one coalesced flush of the accumulated column sums.  Pairs of sparse
 // tiles stay as leftovers, kept in row order and summed per row by a warp with
-// global gathers and atomics, as in the plain kernel.  Within a panel the row sums
-// gather in a shared panel accumulator that is flushed once.
+// global gathers and atomics, as in the plain kernel.  Within a work unit (a run of
+// one panel's tiles) the row sums gather in a shared accumulator that is flushed
+// once.
 //
-// Sums are formed in 64-bit fixed point: each product v x is rounded to an integer
-// multiple of 2^-s and added with integer atomics, which are associative, so the
-// result does not depend on the order in which the pairs land and two runs give
-// bitwise-equal vectors.  s is chosen per call from max |x| and the largest row
-// sum of |H| over both triangles (found during the conversion), so that no sum can
-// exceed 2^62; the rounding error of a sum of m products is below m 2^-(s+1).
+// Shared windows sum in 32-bit fixed point (k_sigma_fx): each product is rounded,
+// by a fixed rule, at a scale chosen per tile from the tile's largest row or column
+// sum of |H|, and integer atomics are associative, so a window's sum does not depend
+// on the order in which the pairs land.  The FP64 sigma (and the FP32 sigma when
+// reproducible sums are asked for) then adds the window sums in 64-bit fixed point
+// (scale 2^s per call, from max |x| and the largest row sum of |H| over both
+// triangles, found during the conversion), so two runs give bitwise-equal vectors.
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -293,7 +295,7 @@ __global__ void k_absmax(const X* __restrict__ x, int64_t n, unsigned long long*
     if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 
-// scalars[0]: max |x| (bits), scalars[1] <- 2^s, scalars[2] <- 2^-s, scalars[3]: panel counter
+// scalars[0]: max |x| (bits), scalars[1] <- 2^s, scalars[2] <- 2^-s, scalars[3]: work-unit counter
 __global__ void k_fixed_scale(double* __restrict__ scalars, double row_abs_max, int smax, int top) {
     const double xmax = __longlong_as_double(*(const long long*)scalars);
     const double bound = row_abs_max * xmax;
@@ -305,37 +307,10 @@ __global__ void k_fixed_scale(double* __restrict__ scalars, double row_abs_max, 
     reinterpret_cast<unsigned long long*>(scalars)[3] = 0ull;
 }
 
-template <typename X>
-__device__ __forceinline__ long long to_fixed(X t, X scale);
-template <>
-__device__ __forceinline__ long long to_fixed<float>(float t, float scale) {
-    return __float2ll_rn(t * scale);
-}
-template <>
-__device__ __forceinline__ long long to_fixed<double>(double t, double scale) {
-    return __double2ll_rn(t * scale);
-}
-
-__device__ __forceinline__ void sadd(long long* a, long long v) {
-    atomicAdd(reinterpret_cast<unsigned long long*>(a), (unsigned long long)v);
-}
-
-// How sigma accumulates (shared windows and the global accumulator).
-// AccExact: 64-bit fixed point, each product rounded by the hardware conversion.
-template <typename X>
-struct AccExact {
-    using T = long long;
-    X scale;
-    __device__ __forceinline__ explicit AccExact(const double* scalars) : scale((X)scalars[1]) {}
-    __device__ __forceinline__ T conv(X t) const { return to_fixed<X>(t, scale); }
-    __device__ __forceinline__ static void add(T* a, T v) { sadd(a, v); }
-};
-// AccFloat: sums in the vector type itself with native atomics (order-dependent).
+// FP32 / FP64 sums added with native global atomics (the window flushes).
 template <typename X>
 struct AccFloat {
     using T = X;
-    __device__ __forceinline__ explicit AccFloat(const double*) {}
-    __device__ __forceinline__ T conv(X t) const { return t; }
     __device__ __forceinline__ static void add(T* a, T v) { atomicAdd(a, v); }
 };
 
@@ -402,27 +377,45 @@ __device__ __forceinline__ void load4(const V* __restrict__ vals, const float* _
     }
 }
 
-// V: stored value type; VLO: add the FP32 remainder (MIXED storage); X: vector type;
-// A: accumulation policy.
-template <typename V, typename X, bool VLO, typename A>
-__global__ void __launch_bounds__(TT) k_sigma_tiles(
+// Fixed-point tile sigma.  Shared-memory integer atomics are single instructions,
+// where FP32 shared atomics are compare-and-swap loops and 64-bit ones slower still
+// (measured on B200: 7.9, 2.6 and 1.5 per clock per SM), so each tile's row and column
+// window sums are formed in 32-bit integers.  Every product is scaled by 2^s_t, s_t
+// chosen from the tile's bound (its largest sum of |H| over one row or one column,
+// times max |x|) so that no window sum exceeds 2^30, and rounded to an integer a
+// (NP = 1), or to a + b 2^-20 with two integers (NP = 2: about 50 significant bits,
+// for FP64 vectors).  Each product is rounded once, by a fixed rule, and integer sums
+// do not depend on their order.  EXACT: the window sums are converted, again by a
+// fixed rule, to the 64-bit fixed point of the whole sigma (scale 2^S, S from the row
+// sums of |H|) and added with 64-bit global atomics, so sigma is bitwise reproducible
+// and ranks' partial sums add exactly; otherwise (FP32 vectors) they are converted to
+// FP32 and added with FP32 vector reductions.  Leftover pairs: one warp per row,
+// private row sum, column sums by global atomics of the rounded products.
+template <typename X, typename V, bool VLO, int NP, bool EXACT>
+__global__ void __launch_bounds__(TT) k_sigma_fx(
     int64_t N, int64_t n_units, const int64_t* __restrict__ units, int rb, int cb,
     const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
-    const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len, const uint32_t* __restrict__ el_idx,
-    const V* __restrict__ vals, const float* __restrict__ vlo, const X* __restrict__ x,
-    typename A::T* __restrict__ acc, double* __restrict__ scalars) {
+    const float* __restrict__ tile_bound, const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len,
+    const uint32_t* __restrict__ el_idx, const V* __restrict__ vals, const float* __restrict__ vlo,
+    const X* __restrict__ x, void* __restrict__ acc_out, double* __restrict__ scalars) {
+    using Y = typename std::conditional<EXACT, long long, X>::type;  // unit row accumulator
     extern __shared__ __align__(16) unsigned char sm[];
     const int R = 1 << rb, C = 1 << cb;
-    using T = typename A::T;
-    T* yP = reinterpret_cast<T*>(sm);
-    T* yJ = yP + R;
-    X* xP = reinterpret_cast<X*>(yJ + C);
+    X* xP = reinterpret_cast<X*>(sm);
     X* xJ = xP + R;
+    Y* yP = reinterpret_cast<Y*>(xJ + C);
+    int* yPa = reinterpret_cast<int*>(yP + R);
+    int* yPb = yPa + R;
+    int* yJa = yPb + (NP == 2 ? R : 0);
+    int* yJb = yJa + C;
     __shared__ long long s_unit;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t cmask = (uint32_t)C - 1u;
-    const A ac(scalars);
+    const double xmax = __longlong_as_double(*reinterpret_cast<const long long*>(scalars));
+    const double gscale = scalars[1];  // 2^S (EXACT)
     unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
+    long long* acc_ll = reinterpret_cast<long long*>(acc_out);
+    X* acc_x = reinterpret_cast<X*>(acc_out);
     for (;;) {
         if (threadIdx.x == 0) s_unit = (long long)atomicAdd(counter, 1ull);
         __syncthreads();
@@ -434,54 +427,93 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
         const int64_t r0 = P << rb;
         const int nr = (int)min((int64_t)R, N - r0);
         stage_window<X>(xP, x + r0, nr);
-        for (int i = threadIdx.x; i < nr; i += TT) yP[i] = 0;
+        for (int i = threadIdx.x; i < R; i += TT) {
+            yP[i] = 0;
+            yPa[i] = 0;
+            if (NP == 2) yPb[i] = 0;
+        }
         __syncthreads();
         for (int64_t t = tb; t < te; t++) {
             const int64_t c0 = (int64_t)tile_win[t] << cb;
             const int w = (int)min((int64_t)C, N - c0);
             const int64_t e0 = tile_off[t];
             const int len = tile_len[t];
+            const double bt = (double)tile_bound[t] * xmax;
+            int sh = 0;
+            if (bt > 0.0 && isfinite(bt)) sh = 29 - ilogb(bt);
+            sh = max(-200, min(200, sh));
+            const X sc = (X)ldexp(1.0, sh);
+            // a window sum (A, B) in the unit of the whole sigma: A 2^(S - s_t) + B 2^(S - s_t - 20)
+            const double fa = ldexp(gscale, -sh), fb = ldexp(gscale, -sh - 20);
+            const X inv = (X)ldexp(1.0, -sh);
             stage_window<X>(xJ, x + c0, w);
-            for (int i = threadIdx.x; i < w; i += TT) yJ[i] = 0;
+            for (int i = threadIdx.x; i < w; i += TT) {
+                yJa[i] = 0;
+                if (NP == 2) yJb[i] = 0;
+            }
             __syncthreads();
-            // the unaligned head and tail one pair per thread, the 16-byte aligned body in
-            // blocks of four consecutive pairs per thread (vector loads, coalesced across the
-            // warp); consecutive pairs of one row add their row sums in a register first
+            // one product to its integer parts
+            auto split = [&](X p, int& a, int& b) {
+                if constexpr (std::is_same<X, double>::value) {
+                    a = __double2int_rn(p);
+                    if (NP == 2) b = __double2int_rn((p - (double)a) * 1048576.0);
+                } else {
+                    a = __float2int_rn(p);
+                    if (NP == 2) b = __float2int_rn((p - (float)a) * 1048576.f);
+                }
+            };
+            auto add_col = [&](uint32_t lc, X p) {
+                int a = 0, b = 0;
+                split(p, a, b);
+                atomicAdd(yJa + lc, a);
+                if (NP == 2) atomicAdd(yJb + lc, b);
+            };
             const int head = (int)min((int64_t)len, (4 - (e0 & 3)) & 3);
             const int64_t eb = e0 + head;
             const int nblk = (len - head) >> 2;
             const int rest = len - head - 4 * nblk;
             if ((int)threadIdx.x < head + rest) {
                 const int64_t e = (int)threadIdx.x < head ? e0 + threadIdx.x : eb + 4 * nblk + (threadIdx.x - head);
-                const uint32_t u = __ldcs(el_idx + e);
+                const uint32_t uu = __ldcs(el_idx + e);
                 X v = (X)__ldcs(vals + e);
                 if constexpr (VLO) v += (X)__ldcs(vlo + e);
-                const uint32_t lr = u >> cb, lc = u & cmask;
+                v *= sc;
+                const uint32_t lr = uu >> cb, lc = uu & cmask;
                 if (lr < (uint32_t)nr && lc < (uint32_t)w) {  // never false for a valid layout
-                    A::add(yP + lr, ac.conv(v * xJ[lc]));
-                    A::add(yJ + lc, ac.conv(v * xP[lr]));
+                    int a = 0, b = 0;
+                    split(v * xJ[lc], a, b);
+                    atomicAdd(yPa + lr, a);
+                    if (NP == 2) atomicAdd(yPb + lr, b);
+                    add_col(lc, v * xP[lr]);
                 }
             }
-            // two blocks per thread and iteration, both loaded before either is summed, so
-            // that every thread keeps two vector loads in flight across the atomics
             auto sum_block = [&](const uint4 u4, const X (&v)[4]) {
-                const uint32_t u[4] = {u4.x, u4.y, u4.z, u4.w};
-                uint32_t rcur = u[0] >> cb;
-                T racc = 0;
+                const uint32_t uq[4] = {u4.x, u4.y, u4.z, u4.w};
+                uint32_t rcur = uq[0] >> cb;
+                int ra = 0, rbb = 0;
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
-                    const uint32_t lr = u[j] >> cb, lc = u[j] & cmask;
+                    const uint32_t lr = uq[j] >> cb, lc = uq[j] & cmask;
                     if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;  // never taken for a valid layout
-                    const T tr = ac.conv(v[j] * xJ[lc]);
-                    A::add(yJ + lc, ac.conv(v[j] * xP[lr]));
+                    const X vs = v[j] * sc;
+                    int a = 0, b = 0;
+                    split(vs * xJ[lc], a, b);
+                    add_col(lc, vs * xP[lr]);
                     if (lr != rcur) {
-                        if (racc != 0 && rcur < (uint32_t)nr) A::add(yP + rcur, racc);
+                        if ((ra | rbb) != 0 && rcur < (uint32_t)nr) {
+                            atomicAdd(yPa + rcur, ra);
+                            if (NP == 2) atomicAdd(yPb + rcur, rbb);
+                        }
                         rcur = lr;
-                        racc = 0;
+                        ra = rbb = 0;
                     }
-                    racc += tr;
+                    ra += a;
+                    rbb += b;
                 }
-                if (racc != 0 && rcur < (uint32_t)nr) A::add(yP + rcur, racc);
+                if ((ra | rbb) != 0 && rcur < (uint32_t)nr) {
+                    atomicAdd(yPa + rcur, ra);
+                    if (NP == 2) atomicAdd(yPb + rcur, rbb);
+                }
             };
             for (int bk = threadIdx.x; bk < nblk; bk += 2 * TT) {
                 const bool two = bk + TT < nblk;
@@ -498,7 +530,41 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
                 if (two) sum_block(u2, v2);
             }
             __syncthreads();
-            flush_window<A>(acc + c0, yJ, w);
+            // column window sums to the global accumulator
+            if constexpr (EXACT) {
+                for (int i = threadIdx.x; i < w; i += TT) {
+                    const int a = yJa[i], b = NP == 2 ? yJb[i] : 0;
+                    if ((a | b) != 0)
+                        atomicAdd(reinterpret_cast<unsigned long long*>(acc_ll + c0 + i),
+                                  (unsigned long long)llrint((double)a * fa + (double)b * fb));
+                }
+            } else {
+                static_assert(EXACT || (std::is_same<X, float>::value && NP == 1), "FP32 sums: one part");
+                if ((reinterpret_cast<uintptr_t>(acc_x + c0) & 15u) == 0) {
+                    for (int i = threadIdx.x; i < (w >> 2); i += TT) {
+                        const int4 a = reinterpret_cast<const int4*>(yJa)[i];
+                        if (a.x | a.y | a.z | a.w)
+                            red_add_v4(reinterpret_cast<float*>(acc_x) + c0 + 4 * i,
+                                       make_float4((float)a.x * (float)inv, (float)a.y * (float)inv,
+                                                   (float)a.z * (float)inv, (float)a.w * (float)inv));
+                    }
+                    for (int i = 4 * (w >> 2) + threadIdx.x; i < w; i += TT)
+                        if (yJa[i] != 0) atomicAdd(acc_x + c0 + i, (X)yJa[i] * inv);
+                } else {
+                    for (int i = threadIdx.x; i < w; i += TT)
+                        if (yJa[i] != 0) atomicAdd(acc_x + c0 + i, (X)yJa[i] * inv);
+                }
+            }
+            // row window sums into the unit's accumulator (row i belongs to this thread here)
+            for (int i = threadIdx.x; i < nr; i += TT) {
+                const int a = yPa[i], b = NP == 2 ? yPb[i] : 0;
+                if ((a | b) != 0) {
+                    if constexpr (EXACT) yP[i] += llrint((double)a * fa + (double)b * fb);
+                    else yP[i] += (X)a * inv;
+                    yPa[i] = 0;
+                    if (NP == 2) yPb[i] = 0;
+                }
+            }
             __syncthreads();
         }
         // leftover pairs: one warp per row, private row sum, column sums by global atomics
@@ -507,201 +573,47 @@ __global__ void __launch_bounds__(TT) k_sigma_tiles(
             const int len = left_len[r0 + i];
             const X xr = xP[i];
             X rs = 0;
-            int k = lane;
-            for (; k + 96 < len; k += 128) {
-                uint32_t q[4];
-                X v[4];
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    q[j] = __ldcs(el_idx + s + k + 32 * j);
-                    v[j] = (X)__ldcs(vals + s + k + 32 * j);
-                    if constexpr (VLO) v[j] += (X)__ldcs(vlo + s + k + 32 * j);
-                }
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    if (q[j] >= (uint64_t)N) continue;  // never taken for a valid layout
-                    rs += v[j] * __ldg(x + q[j]);
-                    A::add(acc + q[j], ac.conv(v[j] * xr));
-                }
-            }
-            for (; k < len; k += 32) {
+            for (int k = lane; k < len; k += 32) {
                 const uint32_t q = __ldcs(el_idx + s + k);
                 X v = (X)__ldcs(vals + s + k);
                 if constexpr (VLO) v += (X)__ldcs(vlo + s + k);
-                if (q >= (uint64_t)N) continue;
+                if (q >= (uint64_t)N) continue;  // never taken for a valid layout
                 rs += v * __ldg(x + q);
-                A::add(acc + q, ac.conv(v * xr));
+                if constexpr (EXACT)
+                    atomicAdd(reinterpret_cast<unsigned long long*>(acc_ll + q),
+                              (unsigned long long)llrint((double)(v * xr) * gscale));
+                else
+                    atomicAdd(acc_x + q, v * xr);
             }
             // fixed lane order: the warp sum does not depend on timing
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(FULL, rs, o);
-            if (lane == 0 && len > 0) A::add(yP + i, ac.conv(rs));
+            if (lane == 0) {
+                if constexpr (EXACT) yP[i] += llrint((double)rs * gscale);
+                else yP[i] += rs;
+            }
         }
         __syncthreads();
-        flush_window<A>(acc + r0, yP, nr);
+        if constexpr (EXACT) {
+            for (int i = threadIdx.x; i < nr; i += TT)
+                if (yP[i] != 0)
+                    atomicAdd(reinterpret_cast<unsigned long long*>(acc_ll + r0 + i), (unsigned long long)yP[i]);
+        } else {
+            flush_window<AccFloat<X>>(acc_x + r0, yP, nr);
+        }
         __syncthreads();
     }
 }
 
-// FP32 sigma with 32-bit integer shared windows.  Shared-memory integer atomics are
-// single instructions, where FP32 shared atomics are compare-and-swap loops, so each
-// tile's row and column window sums are formed in fixed point: every product is
-// rounded to a multiple of 2^-s_t, s_t chosen from the tile's bound (the largest sum
-// of |H| over one row or one column of the tile, times max |x|) so that no window sum
-// exceeds 2^30.  Each product then carries an error of at most 2^-31 of the tile's
-// largest window sum, below FP32 rounding of that sum.  Window sums go to FP32: the
-// row sums into the unit's FP32 row window, the column sums by vector reductions into
-// the global FP32 accumulator.  Leftover pairs as in k_sigma_tiles.
-__global__ void __launch_bounds__(TT) k_sigma_tiles_i32(
-    int64_t N, int64_t n_units, const int64_t* __restrict__ units, int rb, int cb,
-    const int32_t* __restrict__ tile_win, const int32_t* __restrict__ tile_len, const int64_t* __restrict__ tile_off,
-    const float* __restrict__ tile_bound, const int64_t* __restrict__ left_off, const int32_t* __restrict__ left_len,
-    const uint32_t* __restrict__ el_idx, const float* __restrict__ vals, const float* __restrict__ x,
-    float* __restrict__ acc, double* __restrict__ scalars) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    const int R = 1 << rb, C = 1 << cb;
-    float* xP = reinterpret_cast<float*>(sm);
-    float* yP = xP + R;
-    int* yPt = reinterpret_cast<int*>(yP + R);
-    float* xJ = reinterpret_cast<float*>(yPt + R);
-    int* yJ = reinterpret_cast<int*>(xJ + C);
-    __shared__ long long s_unit;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t cmask = (uint32_t)C - 1u;
-    const float xmax = (float)__longlong_as_double(*reinterpret_cast<const long long*>(scalars));
-    unsigned long long* counter = reinterpret_cast<unsigned long long*>(scalars) + 3;
-    for (;;) {
-        if (threadIdx.x == 0) s_unit = (long long)atomicAdd(counter, 1ull);
-        __syncthreads();
-        const int64_t u = s_unit;
-        if (u >= n_units) break;
-        const int64_t tb = units[3 * u], te = units[3 * u + 1], pl = units[3 * u + 2];
-        const int64_t P = pl >> 1;
-        const bool with_left = (pl & 1) != 0;
-        const int64_t r0 = P << rb;
-        const int nr = (int)min((int64_t)R, N - r0);
-        stage_window<float>(xP, x + r0, nr);
-        for (int i = threadIdx.x; i < R; i += TT) {
-            yP[i] = 0.f;
-            yPt[i] = 0;
-        }
-        __syncthreads();
-        for (int64_t t = tb; t < te; t++) {
-            const int64_t c0 = (int64_t)tile_win[t] << cb;
-            const int w = (int)min((int64_t)C, N - c0);
-            const int64_t e0 = tile_off[t];
-            const int len = tile_len[t];
-            // fixed-point scale of this tile: window sums stay below 2^30
-            const float bt = tile_bound[t] * xmax;
-            int sh = 0;
-            if (bt > 0.f && isfinite(bt)) sh = 29 - ilogbf(bt);
-            sh = max(-100, min(100, sh));
-            const float sc = ldexpf(1.f, sh), inv = ldexpf(1.f, -sh);
-            stage_window<float>(xJ, x + c0, w);
-            for (int i = threadIdx.x; i < w; i += TT) yJ[i] = 0;
-            __syncthreads();
-            const int head = (int)min((int64_t)len, (4 - (e0 & 3)) & 3);
-            const int64_t eb = e0 + head;
-            const int nblk = (len - head) >> 2;
-            const int rest = len - head - 4 * nblk;
-            if ((int)threadIdx.x < head + rest) {
-                const int64_t e = (int)threadIdx.x < head ? e0 + threadIdx.x : eb + 4 * nblk + (threadIdx.x - head);
-                const uint32_t uu = __ldcs(el_idx + e);
-                const float v = __ldcs(vals + e) * sc;
-                const uint32_t lr = uu >> cb, lc = uu & cmask;
-                if (lr < (uint32_t)nr && lc < (uint32_t)w) {  // never false for a valid layout
-                    atomicAdd(yPt + lr, __float2int_rn(v * xJ[lc]));
-                    atomicAdd(yJ + lc, __float2int_rn(v * xP[lr]));
-                }
-            }
-            auto sum_block = [&](const uint4 u4, const float4 v4) {
-                const uint32_t uq[4] = {u4.x, u4.y, u4.z, u4.w};
-                const float vq[4] = {v4.x * sc, v4.y * sc, v4.z * sc, v4.w * sc};
-                uint32_t rcur = uq[0] >> cb;
-                int racc = 0;
-#pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const uint32_t lr = uq[j] >> cb, lc = uq[j] & cmask;
-                    if (lr >= (uint32_t)nr || lc >= (uint32_t)w) continue;  // never taken for a valid layout
-                    const int tr = __float2int_rn(vq[j] * xJ[lc]);
-                    atomicAdd(yJ + lc, __float2int_rn(vq[j] * xP[lr]));
-                    if (lr != rcur) {
-                        if (racc != 0 && rcur < (uint32_t)nr) atomicAdd(yPt + rcur, racc);
-                        rcur = lr;
-                        racc = 0;
-                    }
-                    racc += tr;
-                }
-                if (racc != 0 && rcur < (uint32_t)nr) atomicAdd(yPt + rcur, racc);
-            };
-            for (int bk = threadIdx.x; bk < nblk; bk += 2 * TT) {
-                const bool two = bk + TT < nblk;
-                const int64_t e1 = eb + 4 * (int64_t)bk, e2 = e1 + 4 * (int64_t)TT;
-                const uint4 u1 = __ldcs(reinterpret_cast<const uint4*>(el_idx + e1));
-                const float4 v1 = __ldcs(reinterpret_cast<const float4*>(vals + e1));
-                uint4 u2 = make_uint4(0, 0, 0, 0);
-                float4 v2 = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (two) {
-                    u2 = __ldcs(reinterpret_cast<const uint4*>(el_idx + e2));
-                    v2 = __ldcs(reinterpret_cast<const float4*>(vals + e2));
-                }
-                sum_block(u1, v1);
-                if (two) sum_block(u2, v2);
-            }
-            __syncthreads();
-            // column sums to the global accumulator, row sums into the unit's FP32 window
-            if ((reinterpret_cast<uintptr_t>(acc + c0) & 15u) == 0) {
-                for (int i = threadIdx.x; i < (w >> 2); i += TT) {
-                    const int4 a = reinterpret_cast<const int4*>(yJ)[i];
-                    if (a.x | a.y | a.z | a.w)
-                        red_add_v4(acc + c0 + 4 * i, make_float4((float)a.x * inv, (float)a.y * inv,
-                                                                 (float)a.z * inv, (float)a.w * inv));
-                }
-                for (int i = 4 * (w >> 2) + threadIdx.x; i < w; i += TT)
-                    if (yJ[i] != 0) atomicAdd(acc + c0 + i, (float)yJ[i] * inv);
-            } else {
-                for (int i = threadIdx.x; i < w; i += TT)
-                    if (yJ[i] != 0) atomicAdd(acc + c0 + i, (float)yJ[i] * inv);
-            }
-            for (int i = threadIdx.x; i < nr; i += TT) {
-                const int a = yPt[i];
-                if (a != 0) {
-                    yP[i] += (float)a * inv;  // row i belongs to this thread alone here
-                    yPt[i] = 0;
-                }
-            }
-            __syncthreads();
-        }
-        // leftover pairs: one warp per row, private row sum, column sums by global atomics
-        for (int i = warp; with_left && i < nr; i += TT / 32) {
-            const int64_t s = left_off[r0 + i];
-            const int len = left_len[r0 + i];
-            const float xr = xP[i];
-            float rs = 0.f;
-            for (int k = lane; k < len; k += 32) {
-                const uint32_t q = __ldcs(el_idx + s + k);
-                const float v = __ldcs(vals + s + k);
-                if (q >= (uint64_t)N) continue;  // never taken for a valid layout
-                rs += v * __ldg(x + q);
-                atomicAdd(acc + q, v * xr);
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) rs += __shfl_xor_sync(FULL, rs, o);
-            if (lane == 0) yP[i] += rs;  // one warp per row
-        }
-        __syncthreads();
-        flush_window<AccFloat<float>>(acc + r0, yP, nr);
-        __syncthreads();
-    }
-}
-
-// Per tile: the largest sum of |value| over one of its rows or columns (FP32 values),
-// the bound that k_sigma_tiles_i32 scales its fixed point by.
+// Per tile: the largest sum of |value| over one of its rows or columns, the bound that
+// the fixed-point sigma scales each tile by (FP32 values of MIXED storage: the FP32
+// remainder is below 2^-24 of the value, inside the bound's margin).
+template <typename V>
 __global__ void __launch_bounds__(TT) k_tile_bounds(int64_t n_tiles, int rb, int cb,
                                                    const int32_t* __restrict__ tile_len,
                                                    const int64_t* __restrict__ tile_off,
                                                    const uint32_t* __restrict__ el_idx,
-                                                   const float* __restrict__ vals, float* __restrict__ bound) {
+                                                   const V* __restrict__ vals, float* __restrict__ bound) {
     extern __shared__ __align__(16) unsigned char sm[];
     const int R = 1 << rb, C = 1 << cb;
     float* rs = reinterpret_cast<float*>(sm);
@@ -715,7 +627,7 @@ __global__ void __launch_bounds__(TT) k_tile_bounds(int64_t n_tiles, int rb, int
         const int len = tile_len[t];
         for (int k = threadIdx.x; k < len; k += TT) {
             const uint32_t u = el_idx[e0 + k];
-            const float a = fabsf(vals[e0 + k]);
+            const float a = (float)fabs((double)vals[e0 + k]) * (1.f + 0x1p-20f);
             const uint32_t lr = u >> cb, lc = u & cmask;
             if (lr < (uint32_t)R) atomicAdd(rs + lr, a);
             atomicAdd(cs + lc, a);
@@ -849,84 +761,52 @@ inline int grid_n(risqgpu* h, int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)num_sms(h) * 16));
 }
 
-template <typename V, typename X, bool VLO, typename A>
-int launch_tiles_acc(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo, int top) {
-    using T = typename A::T;
+template <typename X, typename V, bool VLO, int NP, bool EXACT>
+int launch_fx(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo) {
+    using Y = typename std::conditional<EXACT, long long, X>::type;
     const int64_t N = (int64_t)h->N;
     const int R = 1 << h->tile_rb, C = 1 << h->tile_cb;
-    const size_t smem = (size_t)(R + C) * (sizeof(T) + sizeof(X));
-    auto kern = k_sigma_tiles<V, X, VLO, A>;
-    const size_t smem_k = smem;
+    const size_t smem = (size_t)(R + C) * sizeof(X) + (size_t)R * sizeof(Y) + (size_t)(R + C) * 4 * NP;
+    auto kern = k_sigma_fx<X, V, VLO, NP, EXACT>;
     static int attr_set[64] = {0};
     const int dev = h->device & 63;
-    if (attr_set[dev] < (int)smem_k) {
-        RQ_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_k));
-        attr_set[dev] = (int)smem_k;
+    if (attr_set[dev] < (int)smem) {
+        RQ_CUDA(h, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set[dev] = (int)smem;
     }
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem_k);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, TT, smem);
     const int grid =
         (int)std::max<int64_t>(1, std::min<int64_t>(h->n_units, (int64_t)num_sms(h) * std::max(occ, 1)));
-    T* acc = reinterpret_cast<T*>(h->d_acc);  // N entries of at most 8 bytes
     RQ_CUDA(h, cudaMemsetAsync(h->d_acc, 0, sizeof(long long) * N, h->stream));
     RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double), h->stream));
     k_absmax<X><<<grid_n(h, N), 256, 0, h->stream>>>(x, N, reinterpret_cast<unsigned long long*>(h->d_sig_scalars));
     k_fixed_scale<<<1, 1, 0, h->stream>>>(h->d_sig_scalars, h->h_row_abs_max,
-                                         std::is_same<X, float>::value ? 100 : 1000, top);
-    kern<<<grid, TT, smem_k, h->stream>>>(N, h->n_units, h->d_units, h->tile_rb, h->tile_cb, h->d_tile_win,
-                                       h->d_tile_len, h->d_tile_off, h->d_left_off, h->d_left_len, h->d_el_idx, vals,
-                                       vlo, x, acc, h->d_sig_scalars);
+                                         std::is_same<X, float>::value ? 100 : 1000, 61);
+    kern<<<grid, TT, smem, h->stream>>>(N, h->n_units, h->d_units, h->tile_rb, h->tile_cb, h->d_tile_win,
+                                       h->d_tile_len, h->d_tile_off, h->d_tile_bound, h->d_left_off, h->d_left_len,
+                                       h->d_el_idx, vals, vlo, x, h->d_acc, h->d_sig_scalars);
     RQ_TRY(check_launch(h, "sigma (tiles)"));
     // with a row-block partition every rank summed its own panels: the exact integer
     // sums are added across the ranks
-    if (h->part_n > 1) RQ_TRY(part_allreduce(h, h->d_acc, (size_t)N));
-    k_fixed_finish<X, T><<<grid_n(h, N), 256, 0, h->stream>>>(N, h->d_diag, x, acc, h->d_sig_scalars, y);
+    if (EXACT && h->part_n > 1) RQ_TRY(part_allreduce(h, h->d_acc, (size_t)N));
+    k_fixed_finish<X, Y><<<grid_n(h, N), 256, 0, h->stream>>>(N, h->d_diag, x, reinterpret_cast<const Y*>(h->d_acc),
+                                                             h->d_sig_scalars, y);
     return check_launch(h, "sigma (tiles)");
 }
 
-int launch_tiles_i32(risqgpu* h, const float* x, float* y) {
-    const int64_t N = (int64_t)h->N;
-    const int R = 1 << h->tile_rb, C = 1 << h->tile_cb;
-    const size_t smem = (size_t)(3 * R + 2 * C) * 4;
-    static int attr_set[64] = {0};
-    const int dev = h->device & 63;
-    if (attr_set[dev] < (int)smem) {
-        RQ_CUDA(h, cudaFuncSetAttribute(k_sigma_tiles_i32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set[dev] = (int)smem;
-    }
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sigma_tiles_i32, TT, smem);
-    const int grid =
-        (int)std::max<int64_t>(1, std::min<int64_t>(h->n_units, (int64_t)num_sms(h) * std::max(occ, 1)));
-    float* acc = reinterpret_cast<float*>(h->d_acc);
-    RQ_CUDA(h, cudaMemsetAsync(h->d_acc, 0, sizeof(long long) * N, h->stream));
-    RQ_CUDA(h, cudaMemsetAsync(h->d_sig_scalars, 0, sizeof(double), h->stream));
-    k_absmax<float><<<grid_n(h, N), 256, 0, h->stream>>>(x, N, reinterpret_cast<unsigned long long*>(h->d_sig_scalars));
-    k_fixed_scale<<<1, 1, 0, h->stream>>>(h->d_sig_scalars, h->h_row_abs_max, 100, 61);
-    k_sigma_tiles_i32<<<grid, TT, smem, h->stream>>>(N, h->n_units, h->d_units, h->tile_rb, h->tile_cb, h->d_tile_win,
-                                                     h->d_tile_len, h->d_tile_off, h->d_tile_bound, h->d_left_off,
-                                                     h->d_left_len, h->d_el_idx, h->d_val32, x, acc,
-                                                     h->d_sig_scalars);
-    RQ_TRY(check_launch(h, "sigma (tiles, FP32)"));
-    k_fixed_finish<float, float><<<grid_n(h, N), 256, 0, h->stream>>>(N, h->d_diag, x, acc, h->d_sig_scalars, y);
-    return check_launch(h, "sigma (tiles, FP32)");
-}
-
-#ifndef RISQ_SIGMA32_I32
-#define RISQ_SIGMA32_I32 1
-#endif
-
-// FP32 vectors sum with 32-bit integer shared windows (k_sigma_tiles_i32) unless the
+// FP32 vectors sum in 32-bit fixed point per tile and FP32 across tiles unless the
 // handle asked for reproducible sums or is partitioned (the ranks' sums must add
-// exactly): those, and FP64 vectors, sum in 64-bit fixed point.
+// exactly); those, and FP64 vectors (two 32-bit parts), add in 64-bit fixed point.
 template <typename V, typename X, bool VLO>
 int launch_tiles(risqgpu* h, const X* x, X* y, const V* vals, const float* vlo) {
-    const bool flt = std::is_same<X, float>::value && !h->reproducible && h->part_n == 1;
     if constexpr (std::is_same<X, float>::value) {
-        if (flt && RISQ_SIGMA32_I32 && h->d_tile_bound) return launch_tiles_i32(h, x, y);
+        if (!h->reproducible && h->part_n == 1)
+            return launch_fx<float, float, false, 1, false>(h, x, y, h->d_val32, nullptr);
+        return launch_fx<float, float, false, 1, true>(h, x, y, h->d_val32, nullptr);
+    } else {
+        return launch_fx<double, V, VLO, 2, true>(h, x, y, vals, vlo);
     }
-    if (flt) return launch_tiles_acc<V, X, VLO, AccFloat<X>>(h, x, y, vals, vlo, 61);
-    return launch_tiles_acc<V, X, VLO, AccExact<X>>(h, x, y, vals, vlo, 61);
 }
 
 // Grow a device array to hold `need` entries, keeping the first `keep`.
@@ -1088,14 +968,24 @@ int TileBuilder::finish() {
         h->n_dense_el = (uint64_t)v;
     }
     RQ_TRY(make_units());
-    if (h->d_val32 && tile_next > 0) {
+    if (tile_next > 0) {
         const int R = 1 << h->tile_rb, C = 1 << h->tile_cb;
         const size_t smem = (size_t)(R + C) * sizeof(float);
         RQ_TRY(dalloc(h, h->d_tile_bound, (size_t)tile_next));
-        RQ_CUDA(h, cudaFuncSetAttribute(k_tile_bounds, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const int grid = (int)std::min<int64_t>(tile_next, (int64_t)num_sms(h) * 8);
-        k_tile_bounds<<<grid, TT, smem, h->stream>>>(tile_next, h->tile_rb, h->tile_cb, h->d_tile_len, h->d_tile_off,
-                                                     h->d_el_idx, h->d_val32, h->d_tile_bound);
+        if (h->d_val64) {
+            RQ_CUDA(h, cudaFuncSetAttribute(k_tile_bounds<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+            k_tile_bounds<double><<<grid, TT, smem, h->stream>>>(tile_next, h->tile_rb, h->tile_cb, h->d_tile_len,
+                                                                 h->d_tile_off, h->d_el_idx, h->d_val64,
+                                                                 h->d_tile_bound);
+        } else {
+            RQ_CUDA(h, cudaFuncSetAttribute(k_tile_bounds<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+            k_tile_bounds<float><<<grid, TT, smem, h->stream>>>(tile_next, h->tile_rb, h->tile_cb, h->d_tile_len,
+                                                                h->d_tile_off, h->d_el_idx, h->d_val32,
+                                                                h->d_tile_bound);
+        }
         RQ_TRY(check_launch(h, "tile bounds"));
     }
     RQ_TRY(dalloc(h, h->d_acc, (size_t)N));
