@@ -58,10 +58,10 @@ CONFIGS = {
 }
 DAV_MAX_ITER = 2000  # the reference's cap of 50 does not converge on these integrals
 # DRAM bytes (read + write) of one FP32 tiled sigma launch from one ncu capture of the
-# kernel on the n20 eps 1e-3 set (profiles/k_sigma_tiles_fp32_n20_eps1e-3.md); the
+# kernel on the n20 eps 1e-3 set (profiles/k_sigma_fx_fp32_n20_eps1e-3.md); the
 # element stream is the traffic and grows with the stored pairs, so a launch over
 # another set is scaled by its pairs
-SIGMA32_CAPTURE = {"pairs": 334_413_323, "dram_bytes": 2_692_757_760 + 6_486_016,
+SIGMA32_CAPTURE = {"pairs": 334_413_323, "dram_bytes": 2_696_127_488 + 11_001_088,
                    "set": "n20 8a8b eps_var 1e-3 seed 0 (551,147 dets)"}
 # The CPU legs time the variational space of the last HCI iteration whose set holds at
 # most this many determinants (the whole set when it is smaller).
@@ -585,7 +585,7 @@ def main():
         "e2e": {"value": N / (e2e * 1e-3), "unit": "dets/s", "ms_per_step": e2e,
                 "h2d_bytes_per_step": int(N * 40), "d2h_bytes_per_step": int(N * 8 + 8)},
         "roofline": {"bound": "hbm",
-                     "kernel": "k_spmv<FP32>" if full_m else "k_sigma_tiles<FP32>",
+                     "kernel": "k_spmv<FP32>" if full_m else "k_sigma_fx<FP32>",
                      "achieved": sig32_gbs, "peak": peak, "unit": "GB/s",
                      "frac": sig32_gbs / peak, "peak_kind": peak_kind,
                      "traffic": None if full_m else
@@ -603,7 +603,7 @@ def main():
                             "legs": {k: {"ms": v[0], "iters": v[1].stats["iters"],
                                          "dE_vs_fp64_uHa": abs(float(v[1].eigenvalues[0]) - e64) * 1e6}
                                      for k, v in legs.items()}},
-        "sigma": {"fp64_kernel": {_capi.FP64: "k_spmv<FP64>", _capi.FP64_UPPER: "k_sigma_tiles<FP64>",
+        "sigma": {"fp64_kernel": {_capi.FP64: "k_spmv<FP64>", _capi.FP64_UPPER: "k_sigma_fx<FP64>",
                                   _capi.COLS: "k_spmv_otf"}[prec64],
                   "fp64_gbs": sig_gbs, "fp64_ms": t_sig, "fp64_frac": sig_gbs / peak,
                   "fp32_gbs": sig32_gbs, "fp32_ms": t_sig32, "fp32_frac": sig32_gbs / peak,
