@@ -229,7 +229,7 @@ RISQGPU_API int risqgpu_set_subspace(risqgpu_t* h, int max_space, int keep);
 /* Reproducible sums for the FP32 sigma of upper-triangle storage.  By default it sums
  * in FP32 with atomic adds, whose order (and so the last bits of the result) varies
  * from run to run; on = 1 makes it sum in 64-bit fixed point like the FP64 sigma,
- * bitwise reproducible, about 30 % slower.  FP64 sigma and partitioned handles always
+ * bitwise reproducible, about 10 % slower.  FP64 sigma and partitioned handles always
  * sum in fixed point.  The reference's serial sums are reproducible by construction
  * (tests/integration_test_suite.rs:413-440). */
 RISQGPU_API int risqgpu_set_reproducible(risqgpu_t* h, int on);
