@@ -184,3 +184,36 @@ def test_parallel_oracle_matches_serial():
     r2 = s2.davidson(1, coeffs, 1e-4, 1e-8, 200, parallel=True)
     assert r1[0] == 0 and r2[0] == 0
     assert abs(r1[1][0] - r2[1][0]) < 1e-10
+
+
+def test_reference_davidson_stays_in_the_spin_flip_even_sector():
+    """On the synthetic n24 10a10b integrals the lowest state of an HCI space is odd
+    under spin flip, while the reference's start vectors (determinants 0 and 1,
+    generate_subspace, davidson.rs:318-338) are even: in exact arithmetic its DPR
+    Davidson stays in the even sector and converges to the second eigenvalue.  A solve
+    whose rounding breaks the symmetry (FP32 sums) can reach the lower, odd state."""
+    import scipy.sparse as sps
+    import scipy.sparse.linalg as sla
+    from risq_b200.fcidump import synthetic_integrals
+    ints = synthetic_integrals(24, 0)
+    oh = O.Ham.from_arrays(ints.norb, 0, ints.nuc, ints.one_body, ints.two_body)
+    hci = O.Hci(oh, 10, 10, 1e-2).set_options(2000)
+    for _ in range(3):
+        hci.step()
+    dets, coeffs, diag = hci.export()
+    n = len(dets)
+    sp = O.Sparse().build(oh, dets, diag, 0)
+    rp, cols, vals, dg = sp.export()
+    U = sps.csr_matrix((vals, (np.repeat(np.arange(n), np.diff(rp)), cols)), shape=(n, n))
+    w, V = sla.eigsh(U + U.T + sps.diags(dg), k=2, which="SA", v0=np.random.default_rng(0).standard_normal(n),
+                     tol=1e-12)
+    order = np.argsort(w)
+    w, V = w[order], V[:, order]
+    key = {tuple(int(v) for v in d): i for i, d in enumerate(dets)}
+    flip = np.array([key[(int(d[2]), int(d[3]), int(d[0]), int(d[1]))] for d in dets])
+    rc, ev, vec, st = sp.davidson(1, None, 1e-4, 1e-8, 2000)
+    assert abs(ev[0] - w[1]) < 1e-7                    # the reference converges to the second state
+    assert w[0] < w[1] - 0.1                           # a lower state exists
+    assert V[:, 0] @ V[flip, 0] < -0.999               # odd under spin flip
+    assert V[:, 1] @ V[flip, 1] > 0.999                # the reference's state is even
+    assert abs(V[0, 0]) < 1e-12 and abs(V[1, 0]) < 1e-12  # no overlap with the start vectors
