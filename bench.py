@@ -276,7 +276,7 @@ def run_reference(args):
     out = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "dets/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": workload_config(args.config, world),
         "cpu_baseline": {"value": v, "unit": "dets/s", "cores": threads, "kind": "port",
                          "sample": f"the variational space of HCI iteration {k} ({n} determinants, {s['nnz']} "
